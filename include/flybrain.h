@@ -1,0 +1,139 @@
+/* flybrain.h - C ABI of the B200 LIF engine (libflybrain.so).
+ *
+ * One engine ("brain") holds B instances ("flies") of a leaky integrate-and-fire network that
+ * share one connectome. It replaces the reference's CPU engine `flyzero.brain.Brain`
+ * (flyzero/brain.py:79-172) and its CuPy engine `flyzero.gpu.BatchBrain`
+ * (flyzero/gpu.py:131-254); the reference binds its engines from Python, so the binding a
+ * maintainer adds is a ctypes stub (INTEGRATION.md shows it).
+ *
+ * Conventions
+ *   - Every function returns FB_OK (0) or an FB_ERR_* code; fb_last_error() gives the message
+ *     of the calling thread's last failure. No C++ exception crosses this boundary.
+ *   - Host pointers are marked [host], device pointers [device]. Device buffers handed out by
+ *     fb_get_views() are owned by the engine and valid until the next fb_set_ext() (ext
+ *     buffers only) or fb_destroy().
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream). All work is enqueued on it;
+ *     no function synchronises the host except where stated.
+ */
+#ifndef FLYBRAIN_H
+#define FLYBRAIN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FB_OK 0
+#define FB_ERR_ARG 1         /* invalid argument (message says which) */
+#define FB_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define FB_ERR_OVERFLOW 3    /* the spike work list overflowed its capacity (device flag) */
+#define FB_ERR_TIMEOUT 4     /* a grid-barrier wait ran out of its iteration budget (device flag) */
+#define FB_ERR_UNSUPPORTED 5 /* valid request that this build does not support */
+
+/* create() flags */
+#define FB_FLAG_F64 1u           /* FP64 state: the oracle-mode step (precision reports) */
+#define FB_FLAG_ACC_FIXED 2u     /* force Q32.32 fixed-point accumulation even for integer counts */
+
+/* schedule: engine kinds */
+#define FB_ENGINE_AUTO 0
+#define FB_ENGINE_STEP 1         /* two launches per simulated step (update, propagate) */
+#define FB_ENGINE_PERSISTENT 2   /* one persistent launch per run; state kept on chip */
+/* schedule: propagation kinds */
+#define FB_PROP_PUSH 0           /* scatter each spiking row into the accumulator (atomics) */
+#define FB_PROP_PULL 1           /* gather per postsynaptic neuron from the spike history */
+
+typedef struct fb_brain fb_brain;
+
+/* LIFParams (flyzero/brain.py:65-76); derived constants follow brain.py:92-96. */
+typedef struct {
+    double v_rest, v_reset, v_th, tau_m, tau_syn, t_ref, delay, w_syn, f_poisson, dt;
+} fb_params;
+
+typedef struct {
+    int64_t n;            /* neurons */
+    int64_t nnz;          /* CSR entries */
+    int32_t batch;        /* instances */
+    int32_t n_delay;      /* max(1, round(delay / dt)) */
+    int32_t n_ref;        /* round(t_ref / dt) */
+    int32_t acc_mode;     /* 0: INT32 synapse counts, 1: INT64 Q32.32 weights */
+    int32_t f64;          /* 1 for FP64 state */
+    int32_t engine;       /* current schedule (FB_ENGINE_*) */
+    int32_t propagation;  /* FB_PROP_* */
+    int32_t lanes;        /* lanes per spike work item (8, 16 or 32) */
+    int32_t group;        /* instances per persistent group (0: persistent engine unavailable) */
+    int32_t ctas;         /* CTAs of the persistent launch */
+    int64_t n_plastic;    /* plastic CSR entries */
+    int64_t n_ext;        /* ext slots (neurons that take Poisson rates and/or bias) */
+    int64_t t;            /* simulated steps since the last full reset (BatchBrain.t) */
+    uint32_t step_no;     /* global step counter feeding the Poisson hash (BatchBrain.step_no) */
+    int64_t launches;     /* kernels launched by this engine so far */
+    int64_t item_capacity;/* spike work items per step list */
+    int64_t bytes_device; /* device memory held by the engine */
+} fb_info;
+
+/* Device views of the mutable state a caller may read and write between runs. */
+typedef struct {
+    void* v;          /* (batch, n) float32, or float64 with FB_FLAG_F64: membrane potential, mV */
+    void* g;          /* (batch, n) same type: synaptic conductance, mV */
+    int8_t* ref;      /* (batch, n) refractory steps left */
+    float* pw;        /* (batch, n_plastic) plastic weights in mV (already x w_syn), gpu.py:163 */
+    float* w0;        /* (n_plastic) initial plastic weights */
+    int32_t* ext_idx; /* (n) ext slot of each neuron or -1 (read-only) */
+    float* p_ext;     /* (batch, n_ext) Poisson probability per step (rate * dt / 1000), gpu.py:226 */
+    float* bias_ext;  /* (batch, n_ext) steady bias, mV (gpu.py:215-220) */
+    int64_t* stop_tick; /* (batch) instance b advances only while t < stop_tick[b] */
+} fb_views;
+
+/* Create an engine. The CSR (pre x post, signed synapse counts as float32, like
+ * flyzero/connectome.py:140-146) is copied to the device, sorted by column within each row.
+ * plastic_pos: CSR positions (Brain.data layout) whose weight is per instance (gpu.py:150-163).
+ * Replaces: Brain.__init__ (flyzero/brain.py:80-102), BatchBrain.__init__ (flyzero/gpu.py:139-184). */
+int fb_create(const fb_params* params, const int64_t* indptr /*[host] n+1*/,
+              const int32_t* indices /*[host] nnz*/, const float* data /*[host] nnz*/, int64_t n,
+              int64_t nnz, int32_t batch, uint32_t seed, const int64_t* plastic_pos /*[host]*/,
+              int64_t n_plastic, uint32_t flags, int32_t device, fb_brain** out);
+
+int fb_destroy(fb_brain* brain);
+
+/* Message of the calling thread's last failure (always NUL-terminated). */
+int fb_last_error(char* buf, int64_t len);
+
+int fb_get_info(const fb_brain* brain, fb_info* out);
+
+int fb_get_views(fb_brain* brain, fb_views* out);
+
+/* Give the neurons idx[0..count) an ext slot if they have none (BatchBrain.slots,
+ * flyzero/gpu.py:201-213). Existing p_ext / bias_ext values are kept; new slots start at 0.
+ * Reallocates p_ext / bias_ext: call fb_get_views() again afterwards. Synchronises the device. */
+int fb_set_ext(fb_brain* brain, const int64_t* idx /*[host]*/, int64_t count);
+
+/* Back to rest: v = v_rest, g = 0, ref = 0 and no synaptic input in flight
+ * (BatchBrain.reset, flyzero/gpu.py:186-199; Brain.reset, flyzero/brain.py:104-110).
+ * flies == NULL or n_flies < 0: every instance, and t = 0. Plastic weights are kept. */
+int fb_reset(fb_brain* brain, const int32_t* flies /*[host]*/, int32_t n_flies, void* stream);
+
+/* Advance every instance `steps` steps (BatchBrain.run, flyzero/gpu.py:228-254; Brain.run,
+ * flyzero/brain.py:133-172).
+ *   counts_out   [device] (batch, n) int32, overwritten with this run's spike counts.
+ *   kicks        [device] NULL: Poisson kicks from the counter hash of p_ext (gpu.py:63-69);
+ *                else a raster (steps, batch, ceil(n_ext/32)) uint32, bit j%32 of word j/32 =
+ *                kick ext slot j at that step (parity mode: identical precomputed input spikes).
+ *   step_counts  [device] NULL or (steps, batch) int32: spikes per step (overwritten).
+ *   step_digest  [device] NULL or (steps, batch) uint64: order-independent raster fingerprint per
+ *                step, the wrapping sum over spiking neurons i of splitmix64(i) (overwritten). */
+int fb_run(fb_brain* brain, int32_t steps, int32_t* counts_out, const uint32_t* kicks,
+           int32_t* step_counts, uint64_t* step_digest, void* stream);
+
+/* Choose the schedule (FB_ENGINE_*, FB_PROP_*, lanes per work item 8/16/32; 0 keeps a field). */
+int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
+
+/* Device error flags raised since the last call (overflow, barrier timeout), then cleared.
+ * Synchronises `stream`. Returns FB_OK or the first raised FB_ERR_* code. */
+int fb_check(fb_brain* brain, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FLYBRAIN_H */
