@@ -1,0 +1,426 @@
+#!/usr/bin/env python
+"""Benchmark: simulated neuron-steps/s of the batched LIF engine on one B200 per rank.
+
+Workload (the batched configuration): 64 instances share the seeded 138,639-neuron synthetic
+connectome (15.1M connections, 54.0M synapses); each has its own seed, grating direction per frame,
+contrast U[0.2, 1], tonic DNp09 drive U[20, 100] Hz, run length U{0.5, 1, 2, 3} s and its own
+plastic weights on the 7,300 inputs of 8 motor neurons. One bench step = one 166-step frame
+(16.64 ms at dt = 0.1 ms) for every instance, i.e. BatchBrain.run(16.64) after the frame's rates
+are written (flyzero/fleet.py:74-81). Inputs (per-frame rates) are resident in HBM before the
+timed region; the working set (state 80 MB + accumulators 71 MB + CSR 94 MB) exceeds the 126 MB L2.
+
+Also reported in the same line: the roofline of the dominant kernel, the plain single-instance
+engine (B=1, two launches per step), the end-to-end path through the public API with host buffers,
+and the CPU oracle port timed on this host. ``--impl reference`` times the CPU port of the
+reference kernel (flyzero/brain.py:32-58) on all host cores, one instance per thread.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (os.path.join(ROOT, "can-the-fly-play-f-zero-_b200"), os.path.join(ROOT, "oracle")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "sim neuron-steps/s (138k LIF, B=64 batched vs B=1 plain) at matched rates"
+UNIT = "neuron-steps/s"
+DT = 0.1
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+BYTES_PER_NEURON_STEP = 26        # v r/w 8 + g r/w 8 + ref r/w 2 + accumulator read+clear 8
+BYTES_PER_SPIKE = 16              # row pointers 8 + count r/w 8
+BYTES_PER_EDGE = 14               # column 4 + count 2 + accumulator read-modify-write 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30, help="timed frames (166 LIF steps each)")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        d = json.load(open(PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(", ") for r in open(self.file.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def workload(batch: int, seed: int):
+    from flyzero_b200 import connectome as cx
+    from flyzero_b200 import workloads as wl
+
+    conn = cx.flywire_scale()
+    drive = wl.grating_drive(conn.n, seed=0, exclude=conn.motor)
+    pos = np.flatnonzero(np.isin(conn.weights.indices, conn.motor))
+    work = wl.BatchedWorkload.make(batch, seed=seed)
+    return conn, drive, pos, work
+
+
+def cpu_baseline(conn, drive, seconds: float) -> dict:
+    """The oracle's restatement of the reference kernel, one thread, on a bounded sample of the
+    same workload (one instance, grating input, frames of 166 steps until ~`seconds` elapse)."""
+    import oracle as O
+    from flyzero_b200 import workloads as wl
+
+    b = O.RefBrain(conn.weights)
+    idx = np.r_[drive.inputs, drive.tonic]
+    rng = np.random.default_rng(1)
+    steps = done = 0
+    busy = 0.0
+    t_ms = 0.0
+    while busy < seconds:
+        rate = np.r_[wl.grating_rates(drive, t_ms, rng.uniform(0, 2 * np.pi)), np.float32(60.0)].astype(np.float32)
+        kicks = O.reference_kicks(int(rng.integers(2 ** 31)), 166, rate * np.float32(DT / 1000.0))
+        t0 = time.perf_counter()
+        b.run_steps(166, idx, kicks)
+        busy += time.perf_counter() - t0
+        steps += 166
+        done += 1
+        t_ms += 166 * DT
+    return {"value": steps * conn.n / busy, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 instance x {steps} steps ({done} frames) of the 138,639-neuron grating workload, "
+                      f"{busy:.1f} s, C port of flyzero/brain.py:32-58 (gcc -O3, AVX2)"}
+
+
+def run_reference(args, world, rank):
+    """CPU port of the reference kernel on all host cores: independent instances, one per thread
+    (the reference's one-fly-per-process model, flyzero/train.py:117-126)."""
+    import oracle as O
+    from flyzero_b200 import connectome as cx
+    from flyzero_b200 import workloads as wl
+
+    if rank != 0:
+        return
+    conn = cx.flywire_scale()
+    drive = wl.grating_drive(conn.n, seed=0, exclude=conn.motor)
+    idx = np.r_[drive.inputs, drive.tonic]
+    threads = len(os.sched_getaffinity(0))
+    b = O.RefBrain(conn.weights)
+    steps = 166
+    rate = np.r_[wl.grating_rates(drive, 0.0, 0.7), np.float32(60.0)].astype(np.float32)
+    kicks = O.reference_kicks(12345, steps, rate * np.float32(DT / 1000.0))
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.ref_pool(threads, threads, b, steps, idx, kicks)
+        dt = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    value = args.steps * threads * steps * conn.n / total
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": "one 166-step frame of the 138,639-neuron grating workload per "
+                                                    "host thread, independent instances", "threads": threads},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{threads} instances x {steps} steps per bench step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def spike_bytes(counts_list, rowlen_dev):
+    """Algorithmic bytes of the spikes in the given count tensors: sum over spikes of 16 + 14 * deg."""
+    import torch
+
+    tot_spk = 0
+    tot_edges = 0
+    for c in counts_list:
+        s = c.sum(0).to(torch.int64)
+        tot_spk += int(s.sum())
+        tot_edges += int((s * rowlen_dev).sum())
+    return tot_spk, tot_edges
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+
+    dev = torch.device("cuda", local)
+    conn, drive, pos, work = workload(args.batch, seed=rank)
+    B, n = args.batch, conn.n
+    fs = wl.frame_steps(DT)
+    frames = args.warmup + args.steps
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=1000 + rank, plastic_pos=pos)
+    idx_in = np.r_[drive.inputs, drive.tonic]
+    j = gb.slots(idx_in).cpu().numpy()
+    assert np.array_equal(np.sort(j), np.arange(len(idx_in))), "inputs own the first ext slots"
+    inv = np.empty_like(j)
+    inv[j] = np.arange(len(j))
+    # per-instance plastic deltas (the reward rule's state after some learning)
+    dw = np.random.default_rng(7 + rank).standard_normal((B, len(pos))).astype(np.float32) * np.float32(0.05)
+    gb.pw += torch.as_tensor(dw, device=dev)
+    gb.set_run_length((work.run_ms / DT).astype(np.int64))
+    # every frame's rates, resident on the device, already in ext-slot order and scaled to p
+    t_ms = 0.0
+    host_rates = np.empty((frames, B, len(idx_in)), np.float32)
+    for f in range(frames):
+        host_rates[f] = work.rates(drive, t_ms, work.directions())[:, inv]
+        t_ms += fs * DT
+    scale = np.float32(DT / 1000.0)
+    p_dev = torch.as_tensor(host_rates, device=dev) * torch.tensor(scale, device=dev)
+    counts = [torch.empty((B, n), dtype=torch.int32, device=dev) for _ in range(frames)]
+    rowlen = torch.as_tensor(np.diff(conn.weights.indptr), device=dev)
+    n_in = len(idx_in)
+    st = torch.cuda.current_stream(dev)
+
+    def frame(f):
+        gb.p_ext[:, :n_in].copy_(p_dev[f])
+        gb.run_steps(fs, counts=counts[f])
+
+    for f in range(args.warmup):
+        frame(f)
+    gb.check()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    launches0 = gb.launches
+    clocks = Clocks(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e_all0, e_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_all0.record(st)
+    for k in range(args.steps):
+        f = args.warmup + k
+        gb.p_ext[:, :n_in].copy_(p_dev[f])
+        ev[k][0].record(st)
+        gb.run_steps(fs, counts=counts[f])
+        ev[k][1].record(st)
+    e_all1.record(st)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(world)
+    gb.check()
+    elapsed_ms = e_all0.elapsed_time(e_all1)
+    kernel_ms = sum(a.elapsed_time(b) for a, b in ev)
+    launches = gb.launches - launches0 + args.steps          # + one p_ext copy kernel per frame
+    t0 = args.warmup * fs
+    stop = (work.run_ms / DT).astype(np.int64)
+    active = int(sum(np.clip(stop - (t0 + k * fs), 0, fs).sum() for k in range(args.steps)))
+    neuron_steps = active * n
+    total_ns = sum_over_ranks(float(neuron_steps), world)
+    max_ms = max_over_ranks(elapsed_ms, world)
+    value = total_ns / (max_ms / 1000.0)
+    spk, edges = spike_bytes(counts[args.warmup:], rowlen)
+    alg_bytes = BYTES_PER_NEURON_STEP * neuron_steps + BYTES_PER_SPIKE * spk + BYTES_PER_EDGE * edges
+    info = gb.info()
+    n_kernel_launches = max(1, launches - args.steps)
+    peak, peak_kind = peaks()
+    achieved = (alg_bytes / n_kernel_launches) / ((kernel_ms / 1000.0) / n_kernel_launches) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
+        "config": {"workload": "batched: 64 instances x 138,639-neuron synthetic connectome, 1 frame = 166 steps "
+                               "at dt 0.1 ms per bench step, grating + tonic Poisson input, 7,300 plastic synapses",
+                   "neurons": n, "connections": int(conn.nnz), "synapses": conn.synapses(), "batch": B,
+                   "steps_per_frame": fs, "active_instance_steps": active, "parallelism": f"replicas x{world}",
+                   "engine": "persistent" if info.group else "step", "group": int(info.group),
+                   "l2": "no flush: working set (state 80 MB + accumulators 71 MB + CSR 94 MB) exceeds the 126 MB L2",
+                   "spikes": spk, "mean_rate_hz": spk / max(1, active) / (DT / 1000.0) / n * 1.0},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "model": "26 B per instance-neuron-step + 16 B per spike + 14 B per edge pushed, per launch of the "
+                              "persistent kernel (one per instance group per frame)"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if not args.no_extras:
+        out["plain_b1"] = plain_b1(conn, drive, dev)
+        out["e2e"] = e2e(gb, host_rates, drive, args, fs, n_in, dev)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(conn, drive, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def plain_b1(conn, drive, dev, frames: int = 6):
+    """The plain single-instance engine: B=1, two launches per step, no persistence, no graph."""
+    import torch
+
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=1, seed=5)
+    gb.set_schedule("step")
+    gb.set_input(np.r_[drive.inputs, drive.tonic], np.r_[wl.grating_rates(drive, 0.0, 0.4), 60.0])
+    fs = wl.frame_steps(DT)
+    for _ in range(2):
+        gb.run_steps(fs)
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = torch.cuda.current_stream(dev)
+    a.record(st)
+    for _ in range(frames):
+        c = gb.run_steps(fs)
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b)
+    return {"value": frames * fs * conn.n / (ms / 1000.0), "unit": UNIT, "engine": "step, B=1, 2 launches/step",
+            "ms_per_frame": ms / frames, "spikes_last_frame": int(c.sum())}
+
+
+def e2e(gb, host_rates, drive, args, fs, n_in, dev):
+    """End to end through the public API with host buffers: per frame, H2D of the frame's rates from
+    pinned memory, the p_ext write (Fleet.think, flyzero/fleet.py:76-77), run(16.64 ms) and a D2H
+    read of the readout DNs' counts (BatchMotor.update reads DN counts, flyzero/batch.py:109)."""
+    import torch
+
+    pinned = torch.as_tensor(host_rates).pin_memory()
+    readout = torch.as_tensor(drive.readout, device=dev)
+    out_h = torch.empty((args.steps, gb.B, len(drive.readout)), dtype=torch.int32).pin_memory()
+    stage = torch.empty((gb.B, n_in), dtype=torch.float32, device=dev)
+    scale = torch.tensor(np.float32(DT / 1000.0), device=dev)
+    st = torch.cuda.current_stream(dev)
+    gb.reset()
+    for f in range(args.warmup):
+        stage.copy_(pinned[f], non_blocking=True)
+        torch.mul(stage, scale, out=gb.p_ext[:, :n_in])
+        c = gb.run(fs * DT)
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for k in range(args.steps):
+        f = args.warmup + k
+        stage.copy_(pinned[f], non_blocking=True)
+        torch.mul(stage, scale, out=gb.p_ext[:, :n_in])
+        c = gb.run(fs * DT)
+        out_h[k].copy_(c.index_select(1, readout), non_blocking=True)
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b)
+    t0 = args.warmup * fs
+    stop = np.asarray(gb.stop_tick.cpu().numpy())
+    active = int(sum(np.clip(stop - (t0 + k * fs), 0, fs).sum() for k in range(args.steps)))
+    return {"value": active * gb.n / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": gb.B * n_in * 4,
+            "d2h_bytes_per_step": gb.B * len(drive.readout) * 4, "ms_per_step": ms / args.steps}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup(args)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,721 @@
+// C ABI of the B200 LIF engine (include/flybrain.h): host orchestration of the kernels in
+// engine.cuh (step engine) and persist.cuh (persistent engine).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "../../include/flybrain.h"
+#include "engine.cuh"
+#include "persist.cuh"
+
+using namespace fb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(FB_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+template <typename T> int dalloc(T** p, size_t count, size_t* total)
+{
+    *p = nullptr;
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    CU(cudaMalloc((void**)p, bytes));
+    *total += bytes;
+    return FB_OK;
+}
+
+template <typename T> int upload(T** p, const std::vector<T>& h, size_t* total)
+{
+    int rc = dalloc(p, h.size(), total);
+    if (rc) return rc;
+    if (!h.empty()) CU(cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return FB_OK;
+}
+
+// FP64 constants computed on the device (exp(-dt/tau) in double), then rounded for FP32 state.
+__global__ void k_consts(double dt, double tau_m, double tau_syn, double f_poisson, double w_syn, double* out)
+{
+    out[0] = exp(-dt / tau_syn);
+    out[1] = dt / tau_m;
+    out[2] = f_poisson * w_syn;
+}
+
+template <typename Real>
+__global__ void k_reset(Real* v, Real* g, int8_t* ref, void* acc0, void* acc1, int acc_bytes, int64_t* pring,
+                        int32_t R, int32_t B, int64_t n, int64_t n_pad, int32_t n_ppost, const uint8_t* fly_mask,
+                        Real v_rest)
+{
+    const int64_t total = (int64_t)B * n;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < total; p += stride) {
+        const int32_t b = (int32_t)(p / n);
+        if (fly_mask && !fly_mask[b]) continue;
+        v[p] = v_rest;
+        g[p] = (Real)0;
+        ref[p] = 0;
+        const int64_t a = (int64_t)b * n_pad + (p - (int64_t)b * n);
+        if (acc_bytes == 4) {
+            ((int32_t*)acc0)[a] = 0;
+            ((int32_t*)acc1)[a] = 0;
+        } else {
+            ((int64_t*)acc0)[a] = 0;
+            ((int64_t*)acc1)[a] = 0;
+        }
+    }
+    const int64_t ptotal = (int64_t)R * B * n_ppost;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < ptotal; p += stride) {
+        const int32_t b = (int32_t)((p / n_ppost) % B);
+        if (fly_mask && !fly_mask[b]) continue;
+        pring[p] = 0;
+    }
+}
+
+__global__ void k_set_ticks(int64_t* reset_tick, const uint8_t* fly_mask, int32_t B, int64_t t)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < B && (!fly_mask || fly_mask[b])) reset_tick[b] = t;
+}
+
+}  // namespace
+
+struct fb_brain {
+    int device = 0;
+    fb_params params{};
+    int64_t n = 0, n_pad = 0, nnz = 0, nnz_pad = 0;
+    int32_t B = 0, n_delay = 1, n_ref = 0, R = 2;
+    int acc_mode = 0;      // 0 INT32 counts, 1 Q32.32
+    int f64 = 0;
+    int contract = 1;
+    uint32_t seed = 0;
+    double consts64[3] = {0, 0, 0};
+    Lif<float> L32{};
+    Lif<double> L64{};
+    // connectome
+    int64_t* rowptr = nullptr;
+    int32_t* col = nullptr;
+    int16_t* cnt = nullptr;
+    int64_t* wfx = nullptr;
+    int32_t max_chunks = 0;
+    // plastic
+    int64_t n_pl = 0;
+    int32_t n_ppost = 0;
+    int64_t* pl_rowptr = nullptr;
+    int32_t* pl_pidx = nullptr;
+    int64_t* pl_q0 = nullptr;
+    int32_t* ppost_of = nullptr;
+    float* pw = nullptr;
+    float* w0 = nullptr;
+    // state
+    void* v = nullptr;
+    void* g = nullptr;
+    int8_t* ref = nullptr;
+    // ext
+    std::vector<int32_t> h_ext_idx;
+    int32_t* ext_idx = nullptr;
+    int64_t n_ext = 0;
+    float* p_ext = nullptr;
+    float* bias_ext = nullptr;
+    std::vector<void*> graveyard;     // superseded buffers, freed at destroy (callers may hold views)
+    // host copy of the CSR (sorted columns) for re-planning the plastic entries
+    std::vector<int64_t> h_ip;
+    std::vector<int32_t> h_ix;
+    std::vector<float> h_wd;          // f32(count * w_syn)
+    std::vector<int64_t> h_pos;       // plastic CSR positions (sorted)
+    std::vector<int32_t> h_ppost_of;  // compact plastic-target index of each neuron, or -1
+    // delay line
+    void* acc[2] = {nullptr, nullptr};
+    int64_t* pring = nullptr;
+    int2* items = nullptr;
+    int32_t* item_count = nullptr;
+    int64_t cap_g = 0;            // items per (step, group) list
+    int32_t list_group = 1;       // instances per list (the persistent group size, or B)
+    int32_t n_groups = 1;
+    unsigned int* bar = nullptr;  // persistent grid-barrier counter
+    int32_t* abort_flag = nullptr;
+    int64_t* reset_tick = nullptr;
+    int64_t* stop_tick = nullptr;
+    uint8_t* fly_mask = nullptr;
+    int32_t* err_h = nullptr;   // host-mapped flags
+    int32_t* err_d = nullptr;
+    // counters
+    int64_t t = 0;
+    uint32_t step_no = 0;
+    int64_t launches = 0;
+    size_t bytes = 0;
+    // schedule
+    int engine = FB_ENGINE_AUTO;
+    int prop = FB_PROP_PUSH;
+    int lanes = 32;
+    int sm_count = 148;
+    PersistPlan plan{};
+
+    DevNet net() const
+    {
+        DevNet N{};
+        N.n = n; N.n_pad = n_pad; N.B = B; N.n_delay = n_delay; N.R = R; N.n_ref = n_ref; N.contract = contract;
+        N.rowptr = rowptr; N.col = col; N.cnt = cnt; N.wfx = wfx;
+        N.n_pl = n_pl; N.n_ppost = n_ppost; N.pl_rowptr = pl_rowptr; N.pl_pidx = pl_pidx; N.pl_q0 = pl_q0;
+        N.ppost_of = ppost_of;
+        N.L32 = L32; N.L64 = L64;
+        return N;
+    }
+    DevState state() const
+    {
+        DevState S{};
+        S.v = v; S.g = g; S.ref = ref; S.pw = pw; S.ext_idx = ext_idx; S.n_ext = (int32_t)n_ext;
+        S.p_ext = p_ext; S.bias_ext = bias_ext; S.acc0 = acc[0]; S.acc1 = acc[1]; S.pring = pring;
+        S.items = items; S.item_count = item_count; S.cap_g = cap_g; S.group = list_group;
+        S.n_groups = n_groups; S.reset_tick = reset_tick;
+        S.stop_tick = stop_tick; S.err = err_d; S.seed = seed;
+        return S;
+    }
+};
+
+namespace {
+
+int free_all(fb_brain* h)
+{
+    void* ptrs[] = {h->rowptr, h->col, h->cnt, h->wfx, h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->pw, h->w0,
+                    h->v, h->g, h->ref, h->ext_idx, h->p_ext, h->bias_ext, h->acc[0], h->acc[1], h->pring,
+                    h->items, h->item_count, h->reset_tick, h->stop_tick, h->fly_mask, h->bar, h->abort_flag};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (void* p : h->graveyard) cudaFree(p);
+    if (h->err_h) cudaFreeHost(h->err_h);
+    return FB_OK;
+}
+
+int64_t py_round(double x) { return (int64_t)std::nearbyint(x); }   // round half to even, like Python
+
+// float weight -> Q32.32, round half to even (x * 2^32 is exact in double)
+int64_t q32_host(float w) { return (int64_t)std::llrint((double)w * 4294967296.0); }
+
+// (Re)build the plastic side for CSR positions `pos` (sorted, unique). Per-instance weights of
+// positions that were plastic before are kept, new ones start at the connectome weight; plastic
+// input in flight is carried over to the new compact target numbering. The device must be idle.
+int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
+{
+    const int64_t n = h->n, n_pl = (int64_t)pos.size();
+    const int32_t B = h->B;
+    std::vector<int64_t> row_of_pos(n_pl);
+    {
+        int64_t r = 0;
+        for (int64_t k = 0; k < n_pl; k++) {
+            while (h->h_ip[r + 1] <= pos[k]) r++;
+            row_of_pos[k] = r;
+        }
+    }
+    std::vector<int64_t> plr(n + 1, 0);
+    std::vector<int32_t> ppost_of(n, -1), pl_pidx(n_pl);
+    std::vector<int64_t> q0(n_pl);
+    std::vector<float> w0(n_pl);
+    std::vector<int32_t> up;
+    up.reserve(n_pl);
+    for (int64_t k = 0; k < n_pl; k++) up.push_back(h->h_ix[pos[k]]);
+    std::sort(up.begin(), up.end());
+    up.erase(std::unique(up.begin(), up.end()), up.end());
+    for (size_t q = 0; q < up.size(); q++) ppost_of[up[q]] = (int32_t)q;
+    const int32_t n_ppost = (int32_t)up.size();
+    for (int64_t k = 0; k < n_pl; k++) {
+        pl_pidx[k] = ppost_of[h->h_ix[pos[k]]];
+        w0[k] = h->h_wd[pos[k]];
+        q0[k] = q32_host(w0[k]);
+        plr[row_of_pos[k] + 1] += 1;
+    }
+    for (int64_t i = 0; i < n; i++) plr[i + 1] += plr[i];
+
+    // per-instance weights: keep the old ones, new entries at w0
+    std::vector<float> pwh((size_t)B * std::max<int64_t>(n_pl, 1));
+    for (int32_t b = 0; b < B; b++) std::copy(w0.begin(), w0.end(), pwh.begin() + (size_t)b * n_pl);
+    if (h->n_pl > 0 && h->pw) {
+        std::vector<float> old((size_t)B * h->n_pl);
+        CU(cudaMemcpy(old.data(), h->pw, old.size() * sizeof(float), cudaMemcpyDeviceToHost));
+        for (int64_t k = 0, j = 0; k < h->n_pl; k++) {
+            while (j < n_pl && pos[j] < h->h_pos[k]) j++;
+            if (j < n_pl && pos[j] == h->h_pos[k])
+                for (int32_t b = 0; b < B; b++) pwh[(size_t)b * n_pl + j] = old[(size_t)b * h->n_pl + k];
+        }
+    }
+    // plastic input in flight, renumbered by target neuron
+    std::vector<int64_t> ring((size_t)h->R * B * std::max(1, n_ppost), 0);
+    if (h->pring && h->n_ppost > 0) {
+        std::vector<int64_t> old((size_t)h->R * B * h->n_ppost);
+        CU(cudaMemcpy(old.data(), h->pring, old.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+        std::vector<int32_t> old_post(h->n_ppost);
+        for (int64_t i = 0; i < n; i++)
+            if (h->h_ppost_of.size() && h->h_ppost_of[i] >= 0) old_post[h->h_ppost_of[i]] = (int32_t)i;
+        for (int64_t r = 0; r < (int64_t)h->R * B; r++)
+            for (int32_t q = 0; q < h->n_ppost; q++) {
+                const int64_t x = old[(size_t)r * h->n_ppost + q];
+                if (x) ring[(size_t)r * n_ppost + ppost_of[old_post[q]]] = x;
+            }
+    }
+    void* olds[] = {h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->w0, h->pring};
+    for (void* p : olds)
+        if (p) cudaFree(p);
+    if (h->pw) h->graveyard.push_back(h->pw);   // callers may still hold a view of the old weights
+    h->pl_rowptr = nullptr; h->pl_pidx = nullptr; h->pl_q0 = nullptr; h->ppost_of = nullptr;
+    h->w0 = nullptr; h->pring = nullptr; h->pw = nullptr;
+    size_t* tb = &h->bytes;
+    int rc;
+    if ((rc = upload(&h->pl_rowptr, plr, tb))) return rc;
+    if ((rc = upload(&h->pl_pidx, pl_pidx, tb))) return rc;
+    if ((rc = upload(&h->pl_q0, q0, tb))) return rc;
+    if ((rc = upload(&h->ppost_of, ppost_of, tb))) return rc;
+    if ((rc = upload(&h->w0, w0, tb))) return rc;
+    if ((rc = upload(&h->pw, pwh, tb))) return rc;
+    if ((rc = upload(&h->pring, ring, tb))) return rc;
+    h->n_pl = n_pl;
+    h->n_ppost = n_ppost;
+    h->h_pos = pos;
+    h->h_ppost_of = std::move(ppost_of);
+    return FB_OK;
+}
+
+int dispatch_step(fb_brain* h, const StepArgs& A, bool raster, bool record, cudaStream_t st);
+int dispatch_push(fb_brain* h, int64_t t, cudaStream_t st);
+
+}  // namespace
+
+extern "C" int fb_last_error(char* buf, int64_t len)
+{
+    if (!buf || len <= 0) return FB_ERR_ARG;
+    std::snprintf(buf, (size_t)len, "%s", g_err.c_str());
+    return FB_OK;
+}
+
+extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_t* indices, const float* data,
+                         int64_t n, int64_t nnz, int32_t batch, uint32_t seed, const int64_t* plastic_pos,
+                         int64_t n_plastic, uint32_t flags, int32_t device, fb_brain** out)
+{
+    if (!out) return fail(FB_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (!P || n <= 0 || nnz < 0 || batch <= 0 || (nnz > 0 && (!indptr || !indices || !data)))
+        return fail(FB_ERR_ARG, "bad connectome arguments (n=%lld nnz=%lld batch=%d)", (long long)n, (long long)nnz, batch);
+    if (n > (int64_t)INT32_MAX - 1) return fail(FB_ERR_ARG, "n=%lld exceeds the int32 neuron index", (long long)n);
+    if (batch >= (1 << (31 - CHUNK_BITS))) return fail(FB_ERR_ARG, "batch %d too large", batch);
+    if (P->dt <= 0 || P->tau_m <= 0 || P->tau_syn <= 0) return fail(FB_ERR_ARG, "dt, tau_m, tau_syn must be > 0");
+    if (indptr && (indptr[0] != 0 || indptr[n] != nnz)) return fail(FB_ERR_ARG, "indptr must start at 0 and end at nnz");
+    CU(cudaSetDevice(device));
+    fb_brain* h = new fb_brain();
+    h->device = device;
+    h->params = *P;
+    h->n = n;
+    h->nnz = nnz;
+    h->B = batch;
+    h->seed = seed;
+    h->f64 = (flags & FB_FLAG_F64) ? 1 : 0;
+    h->n_delay = (int32_t)std::max<int64_t>(1, py_round(P->delay / P->dt));
+    h->n_ref = (int32_t)py_round(P->t_ref / P->dt);
+    h->R = h->n_delay + 1;
+    h->n_pad = (n + 15) / 16 * 16;
+    if (h->n_ref < 0 || h->n_ref > 127) { delete h; return fail(FB_ERR_ARG, "n_ref=%d must fit int8", h->n_ref); }
+    int dev_sms = 0;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
+    h->sm_count = dev_sms > 0 ? dev_sms : 148;
+
+    // --- host CSR: validate, sort columns within rows, classify weights -----------------------
+    std::vector<int64_t> ip(indptr, indptr + n + 1);
+    std::vector<int32_t> ix(nnz);
+    std::vector<float> dv(nnz);
+    bool integral = !(flags & FB_FLAG_ACC_FIXED);
+    {
+        std::vector<int64_t> perm;
+        for (int64_t i = 0; i < n; i++) {
+            const int64_t a = ip[i], b = ip[i + 1];
+            if (b < a) { delete h; return fail(FB_ERR_ARG, "indptr decreases at row %lld", (long long)i); }
+            perm.resize(b - a);
+            for (int64_t k = a; k < b; k++) perm[k - a] = k;
+            std::stable_sort(perm.begin(), perm.end(), [&](int64_t x, int64_t y) { return indices[x] < indices[y]; });
+            for (int64_t k = a; k < b; k++) {
+                const int32_t c = indices[perm[k - a]];
+                if (c < 0 || c >= n) { delete h; return fail(FB_ERR_ARG, "column %d out of range in row %lld", c, (long long)i); }
+                if (k > a && c == ix[k - 1]) { delete h; return fail(FB_ERR_ARG, "duplicate column %d in row %lld", c, (long long)i); }
+                ix[k] = c;
+                dv[k] = data[perm[k - a]];
+            }
+        }
+        for (int64_t k = 0; k < nnz && integral; k++)
+            if (!(dv[k] == std::nearbyint(dv[k])) || std::fabs(dv[k]) > 32767.0f) integral = false;
+    }
+    h->acc_mode = integral ? 0 : 1;
+
+    // plastic positions: sorted, unique, in range
+    std::vector<int64_t> pos(plastic_pos, plastic_pos + std::max<int64_t>(0, n_plastic));
+    std::sort(pos.begin(), pos.end());
+    pos.erase(std::unique(pos.begin(), pos.end()), pos.end());
+    for (int64_t p : pos)
+        if (p < 0 || p >= nnz) { delete h; return fail(FB_ERR_ARG, "plastic position %lld out of range", (long long)p); }
+
+    // weights as the reference scales them: data_f32 = f32(count * f32(w_syn)) (brain.py:89)
+    const float wsyn32 = (float)P->w_syn;
+    std::vector<float> wd(nnz);
+    for (int64_t k = 0; k < nnz; k++) wd[k] = dv[k] * wsyn32;
+
+    // --- padded device CSR (plastic entries keep their connectome weight) -----------------------
+    std::vector<int64_t> rp(n + 1, 0);
+    int64_t max_len = 0;
+    for (int64_t i = 0; i < n; i++) {
+        const int64_t len = ip[i + 1] - ip[i];
+        max_len = std::max(max_len, len);
+        rp[i + 1] = rp[i] + (len + EDGE_ALIGN - 1) / EDGE_ALIGN * EDGE_ALIGN;
+    }
+    h->nnz_pad = rp[n];
+    h->max_chunks = (int32_t)((max_len + CHUNK - 1) / CHUNK);
+    if (h->max_chunks >= (1 << CHUNK_BITS)) { delete h; return fail(FB_ERR_ARG, "a row of %lld entries is too long", (long long)max_len); }
+    std::vector<int32_t> pcol(h->nnz_pad, 0);
+    std::vector<int16_t> pcnt;
+    std::vector<int64_t> pwfx;
+    if (h->acc_mode == 0) pcnt.assign(h->nnz_pad, 0);
+    else pwfx.assign(h->nnz_pad, 0);
+    for (int64_t i = 0; i < n; i++) {
+        int64_t q = rp[i];
+        for (int64_t k = ip[i]; k < ip[i + 1]; k++, q++) {
+            pcol[q] = ix[k];
+            if (h->acc_mode == 0) pcnt[q] = (int16_t)std::nearbyint(dv[k]);
+            else pwfx[q] = q32_host(wd[k]);
+        }
+    }
+    h->h_ip = std::move(ip);
+    h->h_ix = std::move(ix);
+    h->h_wd = std::move(wd);
+
+    // --- device allocations -------------------------------------------------------------------
+    int rc = FB_OK;
+    size_t* tb = &h->bytes;
+#define TRY(x) do { rc = (x); if (rc) { free_all(h); delete h; return rc; } } while (0)
+    TRY(upload(&h->rowptr, rp, tb));
+    TRY(upload(&h->col, pcol, tb));
+    if (h->acc_mode == 0) TRY(upload(&h->cnt, pcnt, tb));
+    else TRY(upload(&h->wfx, pwfx, tb));
+    const size_t nb = (size_t)batch * n;
+    const size_t rs = h->f64 ? sizeof(double) : sizeof(float);
+    TRY(dalloc((char**)&h->v, nb * rs, tb));
+    TRY(dalloc((char**)&h->g, nb * rs, tb));
+    TRY(dalloc(&h->ref, nb, tb));
+    h->h_ext_idx.assign(n, -1);
+    TRY(upload(&h->ext_idx, h->h_ext_idx, tb));
+    TRY(dalloc(&h->p_ext, 1, tb));
+    TRY(dalloc(&h->bias_ext, 1, tb));
+    const size_t ab = h->acc_mode == 0 ? 4 : 8;
+    const size_t nbp = (size_t)batch * h->n_pad;
+    TRY(dalloc((char**)&h->acc[0], nbp * ab, tb));
+    TRY(dalloc((char**)&h->acc[1], nbp * ab, tb));
+    CU(cudaMemset(h->acc[0], 0, nbp * ab));
+    CU(cudaMemset(h->acc[1], 0, nbp * ab));
+    TRY(dalloc(&h->bar, 1, tb));
+    TRY(dalloc(&h->abort_flag, 1, tb));
+    int dev_sms2 = h->sm_count;
+    h->plan = plan_persistent(h->n, h->n_pad, h->B, h->f64 != 0, h->n_ref, (int)ab, dev_sms2, h->device);
+    h->list_group = h->plan.group > 0 ? h->plan.group : h->B;
+    h->n_groups = (h->B + h->list_group - 1) / h->list_group;
+    TRY(install_plastic(h, pos));
+    // worst case: every neuron of every instance fires in the same step
+    int64_t chunks_all = 0;
+    for (int64_t i = 0; i < n; i++) chunks_all += (ip[i + 1] - ip[i] + CHUNK - 1) / CHUNK;
+    h->cap_g = std::max<int64_t>(1, chunks_all * h->list_group);
+    TRY(dalloc(&h->items, (size_t)h->R * h->n_groups * h->cap_g, tb));
+    TRY(dalloc(&h->item_count, (size_t)h->R * h->n_groups, tb));
+    TRY(dalloc(&h->reset_tick, (size_t)batch, tb));
+    TRY(dalloc(&h->stop_tick, (size_t)batch, tb));
+    TRY(dalloc(&h->fly_mask, (size_t)batch, tb));
+    {
+        std::vector<int64_t> st(batch, std::numeric_limits<int64_t>::max());
+        CU(cudaMemcpy(h->stop_tick, st.data(), batch * sizeof(int64_t), cudaMemcpyHostToDevice));
+    }
+    CU(cudaHostAlloc((void**)&h->err_h, 4 * sizeof(int32_t), cudaHostAllocMapped));
+    std::memset(h->err_h, 0, 4 * sizeof(int32_t));
+    CU(cudaHostGetDevicePointer((void**)&h->err_d, h->err_h, 0));
+
+    // FP64 decay factors on the device
+    {
+        double* d = nullptr;
+        CU(cudaMalloc(&d, 3 * sizeof(double)));
+        k_consts<<<1, 1>>>(P->dt, P->tau_m, P->tau_syn, P->f_poisson, P->w_syn, d);
+        CU(cudaGetLastError());
+        CU(cudaMemcpy(h->consts64, d, 3 * sizeof(double), cudaMemcpyDeviceToHost));
+        cudaFree(d);
+        h->launches += 1;
+    }
+    h->L32 = Lif<float>{(float)h->consts64[0], (float)h->consts64[1], (float)h->consts64[2], (float)P->w_syn,
+                        (float)P->v_rest, (float)P->v_th, (float)P->v_reset};
+    h->L64 = Lif<double>{h->consts64[0], h->consts64[1], h->consts64[2], P->w_syn, P->v_rest, P->v_th, P->v_reset};
+    rc = fb_reset(h, nullptr, -1, nullptr);
+    if (rc) { free_all(h); delete h; return rc; }
+    CU(cudaDeviceSynchronize());
+#undef TRY
+    *out = h;
+    return FB_OK;
+}
+
+extern "C" int fb_destroy(fb_brain* h)
+{
+    if (!h) return FB_OK;
+    cudaSetDevice(h->device);
+    cudaDeviceSynchronize();
+    free_all(h);
+    delete h;
+    return FB_OK;
+}
+
+extern "C" int fb_get_info(const fb_brain* h, fb_info* o)
+{
+    if (!h || !o) return fail(FB_ERR_ARG, "NULL argument");
+    std::memset(o, 0, sizeof(*o));
+    o->n = h->n; o->nnz = h->nnz; o->batch = h->B; o->n_delay = h->n_delay; o->n_ref = h->n_ref;
+    o->acc_mode = h->acc_mode; o->f64 = h->f64; o->engine = h->engine; o->propagation = h->prop;
+    o->lanes = h->lanes; o->group = h->plan.group; o->ctas = h->plan.ctas; o->n_plastic = h->n_pl;
+    o->n_ext = h->n_ext; o->t = h->t; o->step_no = h->step_no; o->launches = h->launches;
+    o->item_capacity = h->cap_g; o->bytes_device = (int64_t)h->bytes;
+    o->decay_syn = h->consts64[0]; o->decay_m = h->consts64[1]; o->kick = h->consts64[2];
+    return FB_OK;
+}
+
+extern "C" int fb_get_views(fb_brain* h, fb_views* o)
+{
+    if (!h || !o) return fail(FB_ERR_ARG, "NULL argument");
+    o->v = h->v; o->g = h->g; o->ref = h->ref; o->pw = h->pw; o->w0 = h->w0; o->ext_idx = h->ext_idx;
+    o->p_ext = h->p_ext; o->bias_ext = h->bias_ext; o->stop_tick = h->stop_tick;
+    return FB_OK;
+}
+
+extern "C" int fb_set_ext(fb_brain* h, const int64_t* idx, int64_t count)
+{
+    if (!h || (count > 0 && !idx)) return fail(FB_ERR_ARG, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    std::vector<int64_t> fresh;
+    for (int64_t k = 0; k < count; k++) {
+        if (idx[k] < 0 || idx[k] >= h->n) return fail(FB_ERR_ARG, "neuron %lld out of range", (long long)idx[k]);
+        if (h->h_ext_idx[idx[k]] < 0) fresh.push_back(idx[k]);
+    }
+    std::sort(fresh.begin(), fresh.end());
+    fresh.erase(std::unique(fresh.begin(), fresh.end()), fresh.end());
+    if (fresh.empty()) return FB_OK;
+    const int64_t old = h->n_ext, now = old + (int64_t)fresh.size();
+    for (size_t k = 0; k < fresh.size(); k++) h->h_ext_idx[fresh[k]] = (int32_t)(old + (int64_t)k);
+    CU(cudaDeviceSynchronize());
+    CU(cudaMemcpy(h->ext_idx, h->h_ext_idx.data(), h->n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    float* np_ = nullptr;
+    float* nb_ = nullptr;
+    int rc = dalloc(&np_, (size_t)h->B * now, &h->bytes);
+    if (rc) return rc;
+    rc = dalloc(&nb_, (size_t)h->B * now, &h->bytes);
+    if (rc) return rc;
+    CU(cudaMemset(np_, 0, (size_t)h->B * now * sizeof(float)));
+    CU(cudaMemset(nb_, 0, (size_t)h->B * now * sizeof(float)));
+    if (old > 0) {
+        CU(cudaMemcpy2D(np_, now * sizeof(float), h->p_ext, old * sizeof(float), old * sizeof(float), h->B, cudaMemcpyDeviceToDevice));
+        CU(cudaMemcpy2D(nb_, now * sizeof(float), h->bias_ext, old * sizeof(float), old * sizeof(float), h->B, cudaMemcpyDeviceToDevice));
+    }
+    h->graveyard.push_back(h->p_ext);
+    h->graveyard.push_back(h->bias_ext);
+    h->p_ext = np_;
+    h->bias_ext = nb_;
+    h->n_ext = now;
+    CU(cudaDeviceSynchronize());
+    return FB_OK;
+}
+
+extern "C" int fb_reset(fb_brain* h, const int32_t* flies, int32_t n_flies, void* stream)
+{
+    if (!h) return fail(FB_ERR_ARG, "NULL brain");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool all = (flies == nullptr || n_flies < 0);
+    const uint8_t* mask = nullptr;
+    if (!all) {
+        std::vector<uint8_t> m(h->B, 0);
+        for (int32_t k = 0; k < n_flies; k++) {
+            if (flies[k] < 0 || flies[k] >= h->B) return fail(FB_ERR_ARG, "fly %d out of range", flies[k]);
+            m[flies[k]] = 1;
+        }
+        CU(cudaMemcpyAsync(h->fly_mask, m.data(), h->B, cudaMemcpyHostToDevice, st));
+        CU(cudaStreamSynchronize(st));   // the host vector dies at return
+        mask = h->fly_mask;
+    }
+    const int64_t total = (int64_t)h->B * h->n;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)h->sm_count * 16);
+    const int ab = h->acc_mode == 0 ? 4 : 8;
+    if (h->f64)
+        k_reset<double><<<blocks, 256, 0, st>>>((double*)h->v, (double*)h->g, h->ref, h->acc[0], h->acc[1], ab, h->pring,
+                                                h->R, h->B, h->n, h->n_pad, h->n_ppost, mask, h->params.v_rest);
+    else
+        k_reset<float><<<blocks, 256, 0, st>>>((float*)h->v, (float*)h->g, h->ref, h->acc[0], h->acc[1], ab, h->pring,
+                                               h->R, h->B, h->n, h->n_pad, h->n_ppost, mask, (float)h->params.v_rest);
+    CU(cudaGetLastError());
+    h->launches += 1;
+    if (all) {
+        h->t = 0;
+        CU(cudaMemsetAsync(h->item_count, 0, (size_t)h->R * h->n_groups * sizeof(int32_t), st));
+    }
+    k_set_ticks<<<(h->B + 255) / 256, 256, 0, st>>>(h->reset_tick, mask, h->B, h->t);
+    CU(cudaGetLastError());
+    h->launches += 1;
+    return FB_OK;
+}
+
+extern "C" int fb_set_plastic(fb_brain* h, const int64_t* pos, int64_t count)
+{
+    if (!h || (count > 0 && !pos)) return fail(FB_ERR_ARG, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    std::vector<int64_t> all = h->h_pos;
+    for (int64_t k = 0; k < count; k++) {
+        if (pos[k] < 0 || pos[k] >= h->nnz) return fail(FB_ERR_ARG, "plastic position %lld out of range", (long long)pos[k]);
+        all.push_back(pos[k]);
+    }
+    std::sort(all.begin(), all.end());
+    all.erase(std::unique(all.begin(), all.end()), all.end());
+    if (all.size() == h->h_pos.size()) return FB_OK;
+    CU(cudaDeviceSynchronize());
+    int rc = install_plastic(h, all);
+    if (rc) return rc;
+    CU(cudaDeviceSynchronize());
+    return FB_OK;
+}
+
+extern "C" int fb_set_schedule(fb_brain* h, int32_t engine, int32_t propagation, int32_t lanes)
+{
+    if (!h) return fail(FB_ERR_ARG, "NULL brain");
+    if (engine < 0 || engine > FB_ENGINE_PERSISTENT) return fail(FB_ERR_ARG, "engine %d", engine);
+    if (propagation != FB_PROP_PUSH && propagation != FB_PROP_PULL && propagation != -1)
+        return fail(FB_ERR_ARG, "propagation %d", propagation);
+    if (lanes != 0 && lanes != 8 && lanes != 16 && lanes != 32) return fail(FB_ERR_ARG, "lanes must be 8, 16 or 32");
+    if (engine == FB_ENGINE_PERSISTENT && h->plan.group == 0)
+        return fail(FB_ERR_UNSUPPORTED, "the persistent engine cannot hold one instance of %lld neurons on chip", (long long)h->n);
+    if (propagation == FB_PROP_PULL) return fail(FB_ERR_UNSUPPORTED, "pull propagation is not built in this version");
+    if (engine != 0 || h->engine != 0) h->engine = engine;
+    if (propagation >= 0) h->prop = propagation;
+    if (lanes) h->lanes = lanes;
+    return FB_OK;
+}
+
+extern "C" int fb_check(fb_brain* h, void* stream)
+{
+    if (!h) return fail(FB_ERR_ARG, "NULL brain");
+    CU(cudaSetDevice(h->device));
+    CU(cudaStreamSynchronize((cudaStream_t)stream));
+    const int32_t over = h->err_h[0], tmo = h->err_h[1];
+    h->err_h[0] = h->err_h[1] = 0;
+    if (over) return fail(FB_ERR_OVERFLOW, "spike work list overflowed its capacity of %lld items", (long long)h->cap_g);
+    if (tmo) return fail(FB_ERR_TIMEOUT, "a grid-barrier wait ran out of its budget (step %d)", tmo);
+    return FB_OK;
+}
+
+namespace {
+
+template <typename Real, typename AccT>
+void launch_update(fb_brain* h, const StepArgs& A, bool raster, bool plastic, bool record, int blocks, cudaStream_t st)
+{
+    const DevNet N = h->net();
+    const DevState S = h->state();
+#define L_(R_, P_, C_) k_update<Real, AccT, R_, P_, C_><<<blocks, 256, 0, st>>>(N, S, A)
+    if (raster) {
+        if (plastic) { if (record) L_(true, true, true); else L_(true, true, false); }
+        else { if (record) L_(true, false, true); else L_(true, false, false); }
+    } else {
+        if (plastic) { if (record) L_(false, true, true); else L_(false, true, false); }
+        else { if (record) L_(false, false, true); else L_(false, false, false); }
+    }
+#undef L_
+}
+
+int dispatch_step(fb_brain* h, const StepArgs& A, bool raster, bool record, cudaStream_t st)
+{
+    const int64_t total = (int64_t)h->B * h->n;
+    const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)h->sm_count * 16);
+    const bool plastic = h->n_pl > 0;
+    if (h->f64) {
+        if (h->acc_mode == 0) launch_update<double, int32_t>(h, A, raster, plastic, record, blocks, st);
+        else launch_update<double, int64_t>(h, A, raster, plastic, record, blocks, st);
+    } else {
+        if (h->acc_mode == 0) launch_update<float, int32_t>(h, A, raster, plastic, record, blocks, st);
+        else launch_update<float, int64_t>(h, A, raster, plastic, record, blocks, st);
+    }
+    CU(cudaGetLastError());
+    h->launches += 1;
+    return FB_OK;
+}
+
+template <typename AccT> void launch_push(fb_brain* h, int64_t t, int blocks, cudaStream_t st)
+{
+    const DevNet N = h->net();
+    const DevState S = h->state();
+    if (h->lanes == 8) k_push<AccT, 8><<<blocks, 256, 0, st>>>(N, S, t);
+    else if (h->lanes == 16) k_push<AccT, 16><<<blocks, 256, 0, st>>>(N, S, t);
+    else k_push<AccT, 32><<<blocks, 256, 0, st>>>(N, S, t);
+}
+
+int dispatch_push(fb_brain* h, int64_t t, cudaStream_t st)
+{
+    const int blocks = (int)std::min<int64_t>(std::max<int64_t>(h->sm_count, (int64_t)h->B * 16), (int64_t)h->sm_count * 8);
+    if (h->acc_mode == 0) launch_push<int32_t>(h, t, blocks, st);
+    else launch_push<int64_t>(h, t, blocks, st);
+    CU(cudaGetLastError());
+    h->launches += 1;
+    return FB_OK;
+}
+
+}  // namespace
+
+extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uint32_t* kicks, int32_t* step_counts,
+                      uint64_t* step_digest, void* stream)
+{
+    if (!h || !counts_out) return fail(FB_ERR_ARG, "NULL argument");
+    if (steps < 0) return fail(FB_ERR_ARG, "steps=%d", steps);
+    if (kicks && h->n_ext == 0) return fail(FB_ERR_ARG, "a kick raster needs ext slots");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    CU(cudaMemsetAsync(counts_out, 0, (size_t)h->B * h->n * sizeof(int32_t), st));
+    if (step_counts) CU(cudaMemsetAsync(step_counts, 0, (size_t)steps * h->B * sizeof(int32_t), st));
+    if (step_digest) CU(cudaMemsetAsync(step_digest, 0, (size_t)steps * h->B * sizeof(uint64_t), st));
+    if (steps == 0) return FB_OK;
+    const bool record = step_counts || step_digest;
+    const int32_t words = (int32_t)((h->n_ext + 31) / 32);
+    int engine = h->engine;
+    if (engine == FB_ENGINE_AUTO) engine = (h->plan.group > 0 && !h->f64) ? FB_ENGINE_PERSISTENT : FB_ENGINE_STEP;
+    if (engine == FB_ENGINE_PERSISTENT && h->plan.group > 0 && !h->f64) {
+        PersistArgs P{};
+        P.t0 = h->t; P.step0 = h->step_no; P.steps = steps; P.kicks = kicks; P.words = words;
+        P.counts = counts_out; P.step_counts = step_counts; P.step_digest = step_digest;
+        P.bar = h->bar; P.abort_flag = h->abort_flag;
+        CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
+        int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
+                                   record, h->lanes, st);
+        if (rc) return fail(FB_ERR_CUDA, "persistent launch: %s", cudaGetErrorString((cudaError_t)rc));
+        h->launches += h->plan.launches_per_run;
+    } else {
+        for (int32_t s = 0; s < steps; s++) {
+            StepArgs A{};
+            A.t = h->t + s; A.step_no = h->step_no + (uint32_t)s; A.s = s; A.kicks = kicks; A.words = words;
+            A.counts = counts_out; A.step_counts = step_counts; A.step_digest = step_digest;
+            int rc = dispatch_step(h, A, kicks != nullptr, record, st);
+            if (rc) return rc;
+            rc = dispatch_push(h, A.t, st);
+            if (rc) return rc;
+        }
+    }
+    h->t += steps;
+    h->step_no += (uint32_t)steps;
+    return FB_OK;
+}

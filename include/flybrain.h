@@ -68,8 +68,11 @@ typedef struct {
     int64_t t;            /* simulated steps since the last full reset (BatchBrain.t) */
     uint32_t step_no;     /* global step counter feeding the Poisson hash (BatchBrain.step_no) */
     int64_t launches;     /* kernels launched by this engine so far */
-    int64_t item_capacity;/* spike work items per step list */
+    int64_t item_capacity;/* spike work items per (step, instance group) list */
     int64_t bytes_device; /* device memory held by the engine */
+    double decay_syn;     /* exp(-dt / tau_syn), computed in FP64 on the device */
+    double decay_m;       /* dt / tau_m */
+    double kick;          /* f_poisson * w_syn, mV */
 } fb_info;
 
 /* Device views of the mutable state a caller may read and write between runs. */
@@ -107,6 +110,14 @@ int fb_get_views(fb_brain* brain, fb_views* out);
  * flyzero/gpu.py:201-213). Existing p_ext / bias_ext values are kept; new slots start at 0.
  * Reallocates p_ext / bias_ext: call fb_get_views() again afterwards. Synchronises the device. */
 int fb_set_ext(fb_brain* brain, const int64_t* idx /*[host]*/, int64_t count);
+
+/* Make the CSR positions pos[0..count) plastic as well (per-instance weights in pw), keeping all
+ * state and the synaptic input in flight. A new plastic entry starts at its connectome weight in
+ * every instance; plastic entries always enter as the delta of pw over that weight, pushed at spike
+ * time, so a weight written between runs affects only later spikes (as writes to Brain.data do
+ * in the reference, flyzero/learning.py:130). Reallocates pw / w0: call fb_get_views() again.
+ * Synchronises the device. */
+int fb_set_plastic(fb_brain* brain, const int64_t* pos /*[host]*/, int64_t count);
 
 /* Back to rest: v = v_rest, g = 0, ref = 0 and no synaptic input in flight
  * (BatchBrain.reset, flyzero/gpu.py:186-199; Brain.reset, flyzero/brain.py:104-110).

@@ -31,11 +31,12 @@ typedef struct {
     int32_t contract; /* 1: fuse the two multiply-adds of the step (see lif_oracle_impl.h) */
     const int64_t* indptr;
     const int32_t* indices;
-    const int16_t* cnt; /* acc_mode 0, zero at plastic positions */
-    const int64_t* wfx; /* acc_mode 1, zero at plastic positions */
+    const int16_t* cnt; /* acc_mode 0: signed synapse counts */
+    const int64_t* wfx; /* acc_mode 1: q32(f32(count * w_syn)) */
     int64_t n_pl;
     const int64_t* pl_indptr; /* (n+1) plastic entries grouped by presynaptic neuron */
     const int32_t* pl_post;   /* (n_pl) postsynaptic neuron of each plastic entry */
+    const int64_t* pl_q0;     /* (n_pl) q32 of the entry's connectome weight f32(count * w_syn) */
     const uint8_t* is_ppost;  /* (n) 1 where the neuron receives plastic input */
     float decay_syn_f32, decay_m_f32, kick_f32, w_syn_f32, v_rest_f32, v_th_f32, v_reset_f32;
     double decay_syn_f64, decay_m_f64, kick_f64, w_syn_f64, v_rest_f64, v_th_f64, v_reset_f64;
@@ -89,7 +90,7 @@ int64_t fbo_q32_export(float w) { return fbo_q32(w); }
 /* ------------------------------------------------------------------------------------------
  * Threaded CPU baseline: `n_inst` independent single-instance reference runs (float32,
  * brain.py:32-58) spread over `threads` POSIX threads; each instance has private state and its
- * own kick raster rows. Returns the number of instances completed.
+ * own kick raster rows (or all share one raster). Returns the number of instances completed.
  * ------------------------------------------------------------------------------------------ */
 typedef struct {
     int64_t steps, n, n_in;
@@ -98,7 +99,8 @@ typedef struct {
     const int32_t* indices;
     const float* data;
     const int64_t* input_idx;
-    const uint32_t* kicks; /* (n_inst, steps, words) */
+    const uint32_t* kicks; /* (n_inst, steps, words), or (steps, words) shared when shared_kicks */
+    int32_t shared_kicks;
     float kick, decay_syn, decay_m, v_rest, v_th, v_reset;
     int16_t n_ref;
     int64_t next, n_inst;
@@ -128,7 +130,7 @@ static void* fbo_pool_worker(void* arg)
         memset(pending, 0, sizeof(float) * (size_t)J->n_delay * n);
         memset(counts, 0, sizeof(int32_t) * n);
         fbo_ref_run_f32(J->steps, 0, J->n_delay, n, v, g, ref, pending, counts, J->indptr, J->indices,
-                        J->data, J->input_idx, J->n_in, J->kicks + k * J->steps * words, J->kick,
+                        J->data, J->input_idx, J->n_in, J->kicks + (J->shared_kicks ? 0 : k * J->steps * words), J->kick,
                         J->decay_syn, J->decay_m, J->v_rest, J->v_th, J->v_reset, J->n_ref, bias,
                         1, NULL, NULL);
         for (int64_t i = 0; i < n; i++) local_spikes += counts[i];
@@ -144,7 +146,7 @@ int64_t fbo_ref_pool_f32(int32_t threads, int64_t n_inst, int64_t steps, int32_t
                          const int64_t* indptr, const int32_t* indices, const float* data,
                          const int64_t* input_idx, int64_t n_in, const uint32_t* kicks, float kick,
                          float decay_syn, float decay_m, float v_rest, float v_th, float v_reset,
-                         int16_t n_ref, int64_t* total_spikes)
+                         int16_t n_ref, int32_t shared_kicks, int64_t* total_spikes)
 {
     fbo_pool_job J;
     memset(&J, 0, sizeof(J));
@@ -152,7 +154,7 @@ int64_t fbo_ref_pool_f32(int32_t threads, int64_t n_inst, int64_t steps, int32_t
     J.indptr = indptr; J.indices = indices; J.data = data; J.input_idx = input_idx; J.kicks = kicks;
     J.kick = kick; J.decay_syn = decay_syn; J.decay_m = decay_m;
     J.v_rest = v_rest; J.v_th = v_th; J.v_reset = v_reset; J.n_ref = n_ref;
-    J.next = 0; J.n_inst = n_inst; J.spikes = 0;
+    J.next = 0; J.n_inst = n_inst; J.spikes = 0; J.shared_kicks = shared_kicks;
     pthread_mutex_init(&J.mu, NULL);
     if (threads < 1) threads = 1;
     pthread_t* tid = (pthread_t*)malloc(sizeof(pthread_t) * threads);

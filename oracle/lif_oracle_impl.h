@@ -14,24 +14,42 @@
  * bit j of row s  <=>  `np.random.random() < p_in[j]` at step s of the reference stream.
  * ------------------------------------------------------------------------------------------ */
 int64_t CAT(fbo_ref_run_, SFX)(int64_t steps, int64_t t, int32_t n_delay, int64_t n,
-                               REAL* v, REAL* g, int16_t* ref, REAL* pending, int32_t* counts,
+                               REAL* restrict v, REAL* restrict g, int16_t* restrict ref,
+                               REAL* restrict pending, int32_t* restrict counts,
                                const int64_t* indptr, const int32_t* indices, const REAL* data,
                                const int64_t* input_idx, int64_t n_in, const uint32_t* kicks,
                                REAL kick, REAL decay_syn, REAL decay_m, REAL v_rest, REAL v_th,
-                               REAL v_reset, int16_t n_ref, const REAL* bias, int32_t contract,
+                               REAL v_reset, int16_t n_ref, const REAL* restrict bias, int32_t contract,
                                int32_t* step_counts, uint64_t* step_digest)
 {
     const int64_t words = (n_in + 31) / 32;
     for (int64_t s = 0; s < steps; s++) {
-        REAL* buf = pending + (t % n_delay) * n;
-        for (int64_t i = 0; i < n; i++) {
-            g[i] = contract ? FMA(g[i], decay_syn, buf[i]) : g[i] * decay_syn + buf[i];
-            buf[i] = 0;
-            if (ref[i] > 0) {
-                ref[i] -= 1;
-            } else {
-                REAL e = g[i] + bias[i] - (v[i] - v_rest);
-                v[i] = contract ? FMA(e, decay_m, v[i]) : v[i] + e * decay_m;
+        REAL* restrict buf = pending + (t % n_delay) * n;
+        /* pass 1, if-converted so that it vectorises: the membrane value is computed for every
+         * neuron and kept only where the neuron is not refractory (same per-element operations). */
+        if (contract) {
+            for (int64_t i = 0; i < n; i++) {
+                const REAL gi = FMA(g[i], decay_syn, buf[i]);
+                g[i] = gi;
+                buf[i] = 0;
+                const int16_t r = ref[i];
+                const REAL vo = v[i];
+                const REAL e = gi + bias[i] - (vo - v_rest);
+                const REAL vn = FMA(e, decay_m, vo);
+                v[i] = r > 0 ? vo : vn;
+                ref[i] = (int16_t)(r - (r > 0));
+            }
+        } else {
+            for (int64_t i = 0; i < n; i++) {
+                const REAL gi = g[i] * decay_syn + buf[i];
+                g[i] = gi;
+                buf[i] = 0;
+                const int16_t r = ref[i];
+                const REAL vo = v[i];
+                const REAL e = gi + bias[i] - (vo - v_rest);
+                const REAL vn = vo + e * decay_m;
+                v[i] = r > 0 ? vo : vn;
+                ref[i] = (int16_t)(r - (r > 0));
             }
         }
         if (kicks) {
@@ -66,8 +84,9 @@ int64_t CAT(fbo_ref_run_, SFX)(int64_t steps, int64_t t, int32_t n_delay, int64_
  *   - synaptic input accumulates exactly: INT32 signed synapse counts (acc_mode 0, scaled once:
  *     buf = (REAL)isum * w_syn) or INT64 Q32.32 fixed point for arbitrary float weights
  *     (acc_mode 1: buf = (REAL)(isum * 2^-32));
- *   - plastic weights (per instance, float32) always accumulate in Q32.32 fixed point and are
- *     added after the fixed part: buf = buf + (REAL)(psum * 2^-32);
+ *   - plastic entries keep their connectome weight in the fixed part; each instance's float32
+ *     weight pw enters as a Q32.32 delta over it, q32(pw) - q32(w0), pushed at spike time and
+ *     added after the fixed part: buf = buf + (REAL)(psum * 2^-32) (so pw == w0 adds exactly 0);
  *   - Poisson kicks come from a raster over ext slots (parity) or from the counter hash of the
  *     reference GPU engine (gpu.py:29-31, 63-69): h = mix(tid ^ mix(step*phi ^ mix(seed + b))).
  * All REAL arithmetic is written as separate IEEE operations (this file is compiled with
@@ -166,7 +185,7 @@ int64_t CAT(fbo_engine_run_, SFX)(const fbo_net* net, int64_t steps, int64_t t, 
                     }
                     if (pring) {
                         for (int64_t k = net->pl_indptr[i]; k < net->pl_indptr[i + 1]; k++)
-                            pring[base + net->pl_post[k]] += fbo_q32(pw[b * net->n_pl + k]);
+                            pring[base + net->pl_post[k]] += fbo_q32(pw[b * net->n_pl + k]) - net->pl_q0[k];
                     }
                 }
             }

@@ -13,7 +13,8 @@ What it restates (file:line in the reference project):
   (brain.py:34, :46-48); numba's generator is NumPy's legacy MT19937, so the kick raster of a
   run is ``RandomState(seed_k).random_sample((steps, n_in)) < p_in``.
 * ``EngineOracle``: the batched engine's semantics (``flyzero/gpu.py:33-118`` order of
-  operations, exact INT32 / Q32.32 accumulation, ext slots, per-instance plastic weights).
+  operations, exact INT32 / Q32.32 accumulation, ext slots, per-instance plastic weights
+  entering as Q32.32 deltas over the connectome weight).
 * ``reward_step`` / ``batch_reward_step``: ``flyzero/learning.py:116-131`` and
   ``flyzero/batch.py:158-172, 482-495`` in NumPy.
 """
@@ -46,7 +47,8 @@ class _Net(C.Structure):
     _fields_ = [("n", C.c_int64), ("nnz", C.c_int64), ("B", C.c_int64),
                 ("n_delay", C.c_int32), ("n_ref", C.c_int32), ("acc_mode", C.c_int32), ("contract", C.c_int32),
                 ("indptr", i64p), ("indices", i32p), ("cnt", i16p), ("wfx", i64p),
-                ("n_pl", C.c_int64), ("pl_indptr", i64p), ("pl_post", i32p), ("is_ppost", u8p)] + \
+                ("n_pl", C.c_int64), ("pl_indptr", i64p), ("pl_post", i32p), ("pl_q0", i64p),
+                ("is_ppost", u8p)] + \
                [(f"{k}_f32", C.c_float) for k in ("decay_syn", "decay_m", "kick", "w_syn", "v_rest", "v_th", "v_reset")] + \
                [(f"{k}_f64", C.c_double) for k in ("decay_syn", "decay_m", "kick", "w_syn", "v_rest", "v_th", "v_reset")]
 
@@ -76,7 +78,7 @@ def lib():
         L.fbo_ref_pool_f32.restype = C.c_int64
         L.fbo_ref_pool_f32.argtypes = [C.c_int32, C.c_int64, C.c_int64, C.c_int32, C.c_int64, i64p, i32p, f32p,
                                        i64p, C.c_int64, u32p, C.c_float, C.c_float, C.c_float, C.c_float,
-                                       C.c_float, C.c_float, C.c_int16, i64p]
+                                       C.c_float, C.c_float, C.c_int16, C.c_int32, i64p]
         L.fbo_spike_tag_export.restype = C.c_uint64
         L.fbo_spike_tag_export.argtypes = [C.c_uint64]
         L.fbo_mix32_export.restype = C.c_uint32
@@ -247,13 +249,9 @@ class EngineOracle:
             acc_mode = "count" if integral_counts(raw) else "fixed"
         self.acc_mode = acc_mode
         if acc_mode == "count":
-            cnt = np.rint(raw).astype(np.int16)
-            cnt[pos] = 0
-            self.cnt, self.wfx = cnt, None
+            self.cnt, self.wfx = np.rint(raw).astype(np.int16), None
         else:
-            wfx = q32(self.data)
-            wfx[pos] = 0
-            self.cnt, self.wfx = None, wfx
+            self.cnt, self.wfx = None, q32(self.data)
         rows = np.repeat(np.arange(n), np.diff(self.indptr))
         self.pl_pre = rows[pos]
         self.pl_post = self.indices[pos].astype(np.int32)
@@ -261,6 +259,7 @@ class EngineOracle:
         self.is_ppost = np.zeros(n, np.uint8)
         self.is_ppost[self.pl_post] = 1
         self.w0 = self.data[pos].copy()
+        self.pl_q0 = q32(self.w0)
         self.pw = np.tile(self.w0, (batch, 1)).astype(np.float32)
         self.n_delay, self.n_ref = p.n_delay, p.n_ref
         self.seed = np.uint32(seed)
@@ -279,7 +278,7 @@ class EngineOracle:
                    acc_mode=0 if self.acc_mode == "count" else 1, contract=int(self.contract),
                    indptr=_p(self.indptr, i64p), indices=_p(self.indices, i32p), cnt=_p(self.cnt, i16p),
                    wfx=_p(self.wfx, i64p), n_pl=len(self.plastic_pos), pl_indptr=_p(self.pl_indptr, i64p),
-                   pl_post=_p(self.pl_post, i32p), is_ppost=_p(self.is_ppost, u8p),
+                   pl_post=_p(self.pl_post, i32p), pl_q0=_p(self.pl_q0, i64p), is_ppost=_p(self.is_ppost, u8p),
                    decay_syn_f32=ds32, decay_m_f32=dm32, kick_f32=k32, w_syn_f32=np.float32(p.w_syn),
                    v_rest_f32=np.float32(p.v_rest), v_th_f32=np.float32(p.v_th), v_reset_f32=np.float32(p.v_reset),
                    decay_syn_f64=ds64, decay_m_f64=dm64, kick_f64=k64, w_syn_f64=float(p.w_syn),
@@ -294,6 +293,16 @@ class EngineOracle:
         self.ring = np.zeros((self.n_delay, B, n), np.int32 if self.acc_mode == "count" else np.int64)
         self.pring = np.zeros((self.n_delay, B, n), np.int64) if len(self.plastic_pos) else None
         self.t = 0
+
+    def reset_flies(self, flies):
+        """BatchBrain.reset(flies) (gpu.py:195-199): rest state, no input in flight."""
+        f = np.atleast_1d(np.asarray(flies, np.int64))
+        self.v[f] = self.p.v_rest
+        self.g[f] = 0
+        self.ref[f] = 0
+        self.ring[:, f] = 0
+        if self.pring is not None:
+            self.pring[:, f] = 0
 
     def slots(self, idx):
         idx = np.asarray(idx, np.int64).ravel()
@@ -331,17 +340,19 @@ class EngineOracle:
 
 
 def ref_pool(threads: int, n_inst: int, brain: RefBrain, steps: int, input_idx, kicks) -> int:
-    """Threaded CPU baseline: ``n_inst`` independent reference runs of ``steps`` steps
-    (``kicks``: (n_inst, steps, n_in) bool). Returns the total spike count."""
+    """Threaded CPU baseline: ``n_inst`` independent reference runs of ``steps`` steps, one
+    instance per thread at a time (``kicks``: (n_inst, steps, n_in) bool, or (steps, n_in) shared
+    by all instances). Returns the total spike count."""
     L = lib()
     idx = np.asarray(input_idx, np.int64)
+    shared = kicks.ndim == 2
     packed = np.ascontiguousarray(pack_bits(kicks))
     total = np.zeros(1, np.int64)
     b = brain
     L.fbo_ref_pool_f32(threads, n_inst, steps, b.n_delay, b.n, _p(b.indptr, i64p), _p(b.indices, i32p),
                        _p(b.data, f32p), _p(idx, i64p), len(idx), _p(packed, u32p), b.kick, b.decay_syn,
                        b.decay_m, np.float32(b.p.v_rest), np.float32(b.p.v_th), np.float32(b.p.v_reset),
-                       b.n_ref, _p(total, i64p))
+                       b.n_ref, int(shared), _p(total, i64p))
     return int(total[0])
 
 
