@@ -11,6 +11,7 @@
 
 #include "../../include/flybrain.h"
 #include "engine.cuh"
+#include "host_prep.hpp"
 #include "persist.cuh"
 
 using namespace fb;
@@ -137,12 +138,8 @@ struct fb_brain {
     float* p_ext = nullptr;
     float* bias_ext = nullptr;
     std::vector<void*> graveyard;     // superseded buffers, freed at destroy (callers may hold views)
-    // host copy of the CSR (sorted columns) for re-planning the plastic entries
-    std::vector<int64_t> h_ip;
-    std::vector<int32_t> h_ix;
-    std::vector<float> h_wd;          // f32(count * w_syn)
-    std::vector<int64_t> h_pos;       // plastic CSR positions (sorted)
-    std::vector<int32_t> h_ppost_of;  // compact plastic-target index of each neuron, or -1
+    HostCsr hc;                       // host copy of the CSR for re-planning the plastic entries
+    PlasticPlan plastic;              // current plastic plan
     // delay line
     void* acc[2] = {nullptr, nullptr};
     int64_t* pring = nullptr;
@@ -208,69 +205,24 @@ int free_all(fb_brain* h)
 
 int64_t py_round(double x) { return (int64_t)std::nearbyint(x); }   // round half to even, like Python
 
-// float weight -> Q32.32, round half to even (x * 2^32 is exact in double)
-int64_t q32_host(float w) { return (int64_t)std::llrint((double)w * 4294967296.0); }
-
-// (Re)build the plastic side for CSR positions `pos` (sorted, unique). Per-instance weights of
-// positions that were plastic before are kept, new ones start at the connectome weight; plastic
-// input in flight is carried over to the new compact target numbering. The device must be idle.
+// (Re)build the plastic side for CSR positions `pos`. Per-instance weights of positions that
+// were plastic before are kept, new ones start at the connectome weight; plastic input in flight
+// is carried over to the new compact target numbering. The device must be idle.
 int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
 {
-    const int64_t n = h->n, n_pl = (int64_t)pos.size();
+    PlasticPlan P;
+    std::string err = plan_plastic(h->hc, pos, P);
+    if (!err.empty()) return fail(FB_ERR_ARG, "%s", err.c_str());
     const int32_t B = h->B;
-    std::vector<int64_t> row_of_pos(n_pl);
-    {
-        int64_t r = 0;
-        for (int64_t k = 0; k < n_pl; k++) {
-            while (h->h_ip[r + 1] <= pos[k]) r++;
-            row_of_pos[k] = r;
-        }
-    }
-    std::vector<int64_t> plr(n + 1, 0);
-    std::vector<int32_t> ppost_of(n, -1), pl_pidx(n_pl);
-    std::vector<int64_t> q0(n_pl);
-    std::vector<float> w0(n_pl);
-    std::vector<int32_t> up;
-    up.reserve(n_pl);
-    for (int64_t k = 0; k < n_pl; k++) up.push_back(h->h_ix[pos[k]]);
-    std::sort(up.begin(), up.end());
-    up.erase(std::unique(up.begin(), up.end()), up.end());
-    for (size_t q = 0; q < up.size(); q++) ppost_of[up[q]] = (int32_t)q;
-    const int32_t n_ppost = (int32_t)up.size();
-    for (int64_t k = 0; k < n_pl; k++) {
-        pl_pidx[k] = ppost_of[h->h_ix[pos[k]]];
-        w0[k] = h->h_wd[pos[k]];
-        q0[k] = q32_host(w0[k]);
-        plr[row_of_pos[k] + 1] += 1;
-    }
-    for (int64_t i = 0; i < n; i++) plr[i + 1] += plr[i];
-
-    // per-instance weights: keep the old ones, new entries at w0
-    std::vector<float> pwh((size_t)B * std::max<int64_t>(n_pl, 1));
-    for (int32_t b = 0; b < B; b++) std::copy(w0.begin(), w0.end(), pwh.begin() + (size_t)b * n_pl);
-    if (h->n_pl > 0 && h->pw) {
-        std::vector<float> old((size_t)B * h->n_pl);
-        CU(cudaMemcpy(old.data(), h->pw, old.size() * sizeof(float), cudaMemcpyDeviceToHost));
-        for (int64_t k = 0, j = 0; k < h->n_pl; k++) {
-            while (j < n_pl && pos[j] < h->h_pos[k]) j++;
-            if (j < n_pl && pos[j] == h->h_pos[k])
-                for (int32_t b = 0; b < B; b++) pwh[(size_t)b * n_pl + j] = old[(size_t)b * h->n_pl + k];
-        }
-    }
-    // plastic input in flight, renumbered by target neuron
-    std::vector<int64_t> ring((size_t)h->R * B * std::max(1, n_ppost), 0);
+    std::vector<float> old_pw((size_t)B * h->n_pl);
+    if (h->n_pl > 0) CU(cudaMemcpy(old_pw.data(), h->pw, old_pw.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    std::vector<float> pwh = remap_weights(h->plastic, old_pw, P, B);
+    std::vector<int64_t> old_ring;
     if (h->pring && h->n_ppost > 0) {
-        std::vector<int64_t> old((size_t)h->R * B * h->n_ppost);
-        CU(cudaMemcpy(old.data(), h->pring, old.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
-        std::vector<int32_t> old_post(h->n_ppost);
-        for (int64_t i = 0; i < n; i++)
-            if (h->h_ppost_of.size() && h->h_ppost_of[i] >= 0) old_post[h->h_ppost_of[i]] = (int32_t)i;
-        for (int64_t r = 0; r < (int64_t)h->R * B; r++)
-            for (int32_t q = 0; q < h->n_ppost; q++) {
-                const int64_t x = old[(size_t)r * h->n_ppost + q];
-                if (x) ring[(size_t)r * n_ppost + ppost_of[old_post[q]]] = x;
-            }
+        old_ring.resize((size_t)h->R * B * h->n_ppost);
+        CU(cudaMemcpy(old_ring.data(), h->pring, old_ring.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
     }
+    std::vector<int64_t> ring = remap_ring(h->plastic, old_ring, P, (int64_t)h->R * B);
     void* olds[] = {h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->w0, h->pring};
     for (void* p : olds)
         if (p) cudaFree(p);
@@ -279,17 +231,16 @@ int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
     h->w0 = nullptr; h->pring = nullptr; h->pw = nullptr;
     size_t* tb = &h->bytes;
     int rc;
-    if ((rc = upload(&h->pl_rowptr, plr, tb))) return rc;
-    if ((rc = upload(&h->pl_pidx, pl_pidx, tb))) return rc;
-    if ((rc = upload(&h->pl_q0, q0, tb))) return rc;
-    if ((rc = upload(&h->ppost_of, ppost_of, tb))) return rc;
-    if ((rc = upload(&h->w0, w0, tb))) return rc;
+    if ((rc = upload(&h->pl_rowptr, P.plr, tb))) return rc;
+    if ((rc = upload(&h->pl_pidx, P.pl_pidx, tb))) return rc;
+    if ((rc = upload(&h->pl_q0, P.q0, tb))) return rc;
+    if ((rc = upload(&h->ppost_of, P.ppost_of, tb))) return rc;
+    if ((rc = upload(&h->w0, P.w0, tb))) return rc;
     if ((rc = upload(&h->pw, pwh, tb))) return rc;
     if ((rc = upload(&h->pring, ring, tb))) return rc;
-    h->n_pl = n_pl;
-    h->n_ppost = n_ppost;
-    h->h_pos = pos;
-    h->h_ppost_of = std::move(ppost_of);
+    h->n_pl = P.n_pl;
+    h->n_ppost = P.n_ppost;
+    h->plastic = std::move(P);
     return FB_OK;
 }
 
@@ -311,12 +262,11 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
 {
     if (!out) return fail(FB_ERR_ARG, "out is NULL");
     *out = nullptr;
-    if (!P || n <= 0 || nnz < 0 || batch <= 0 || (nnz > 0 && (!indptr || !indices || !data)))
+    if (!P || n <= 0 || nnz < 0 || batch <= 0 || !indptr || (nnz > 0 && (!indices || !data)))
         return fail(FB_ERR_ARG, "bad connectome arguments (n=%lld nnz=%lld batch=%d)", (long long)n, (long long)nnz, batch);
     if (n > (int64_t)INT32_MAX - 1) return fail(FB_ERR_ARG, "n=%lld exceeds the int32 neuron index", (long long)n);
     if (batch >= (1 << (31 - CHUNK_BITS))) return fail(FB_ERR_ARG, "batch %d too large", batch);
     if (P->dt <= 0 || P->tau_m <= 0 || P->tau_syn <= 0) return fail(FB_ERR_ARG, "dt, tau_m, tau_syn must be > 0");
-    if (indptr && (indptr[0] != 0 || indptr[n] != nnz)) return fail(FB_ERR_ARG, "indptr must start at 0 and end at nnz");
     CU(cudaSetDevice(device));
     fb_brain* h = new fb_brain();
     h->device = device;
@@ -335,80 +285,26 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, device);
     h->sm_count = dev_sms > 0 ? dev_sms : 148;
 
-    // --- host CSR: validate, sort columns within rows, classify weights -----------------------
-    std::vector<int64_t> ip(indptr, indptr + n + 1);
-    std::vector<int32_t> ix(nnz);
-    std::vector<float> dv(nnz);
-    bool integral = !(flags & FB_FLAG_ACC_FIXED);
+    // --- host CSR: validate, sort columns within rows, classify weights, pad rows ------------
     {
-        std::vector<int64_t> perm;
-        for (int64_t i = 0; i < n; i++) {
-            const int64_t a = ip[i], b = ip[i + 1];
-            if (b < a) { delete h; return fail(FB_ERR_ARG, "indptr decreases at row %lld", (long long)i); }
-            perm.resize(b - a);
-            for (int64_t k = a; k < b; k++) perm[k - a] = k;
-            std::stable_sort(perm.begin(), perm.end(), [&](int64_t x, int64_t y) { return indices[x] < indices[y]; });
-            for (int64_t k = a; k < b; k++) {
-                const int32_t c = indices[perm[k - a]];
-                if (c < 0 || c >= n) { delete h; return fail(FB_ERR_ARG, "column %d out of range in row %lld", c, (long long)i); }
-                if (k > a && c == ix[k - 1]) { delete h; return fail(FB_ERR_ARG, "duplicate column %d in row %lld", c, (long long)i); }
-                ix[k] = c;
-                dv[k] = data[perm[k - a]];
-            }
-        }
-        for (int64_t k = 0; k < nnz && integral; k++)
-            if (!(dv[k] == std::nearbyint(dv[k])) || std::fabs(dv[k]) > 32767.0f) integral = false;
+        std::string err = prepare_csr(indptr, indices, data, n, nnz, (float)P->w_syn,
+                                      (flags & FB_FLAG_ACC_FIXED) != 0, h->hc);
+        if (!err.empty()) { delete h; return fail(FB_ERR_ARG, "%s", err.c_str()); }
     }
-    h->acc_mode = integral ? 0 : 1;
-
-    // plastic positions: sorted, unique, in range
+    const HostCsr& H = h->hc;
+    h->acc_mode = H.acc_mode;
+    h->nnz_pad = H.nnz_pad;
+    h->max_chunks = H.max_chunks;
     std::vector<int64_t> pos(plastic_pos, plastic_pos + std::max<int64_t>(0, n_plastic));
-    std::sort(pos.begin(), pos.end());
-    pos.erase(std::unique(pos.begin(), pos.end()), pos.end());
-    for (int64_t p : pos)
-        if (p < 0 || p >= nnz) { delete h; return fail(FB_ERR_ARG, "plastic position %lld out of range", (long long)p); }
-
-    // weights as the reference scales them: data_f32 = f32(count * f32(w_syn)) (brain.py:89)
-    const float wsyn32 = (float)P->w_syn;
-    std::vector<float> wd(nnz);
-    for (int64_t k = 0; k < nnz; k++) wd[k] = dv[k] * wsyn32;
-
-    // --- padded device CSR (plastic entries keep their connectome weight) -----------------------
-    std::vector<int64_t> rp(n + 1, 0);
-    int64_t max_len = 0;
-    for (int64_t i = 0; i < n; i++) {
-        const int64_t len = ip[i + 1] - ip[i];
-        max_len = std::max(max_len, len);
-        rp[i + 1] = rp[i] + (len + EDGE_ALIGN - 1) / EDGE_ALIGN * EDGE_ALIGN;
-    }
-    h->nnz_pad = rp[n];
-    h->max_chunks = (int32_t)((max_len + CHUNK - 1) / CHUNK);
-    if (h->max_chunks >= (1 << CHUNK_BITS)) { delete h; return fail(FB_ERR_ARG, "a row of %lld entries is too long", (long long)max_len); }
-    std::vector<int32_t> pcol(h->nnz_pad, 0);
-    std::vector<int16_t> pcnt;
-    std::vector<int64_t> pwfx;
-    if (h->acc_mode == 0) pcnt.assign(h->nnz_pad, 0);
-    else pwfx.assign(h->nnz_pad, 0);
-    for (int64_t i = 0; i < n; i++) {
-        int64_t q = rp[i];
-        for (int64_t k = ip[i]; k < ip[i + 1]; k++, q++) {
-            pcol[q] = ix[k];
-            if (h->acc_mode == 0) pcnt[q] = (int16_t)std::nearbyint(dv[k]);
-            else pwfx[q] = q32_host(wd[k]);
-        }
-    }
-    h->h_ip = std::move(ip);
-    h->h_ix = std::move(ix);
-    h->h_wd = std::move(wd);
 
     // --- device allocations -------------------------------------------------------------------
     int rc = FB_OK;
     size_t* tb = &h->bytes;
 #define TRY(x) do { rc = (x); if (rc) { free_all(h); delete h; return rc; } } while (0)
-    TRY(upload(&h->rowptr, rp, tb));
-    TRY(upload(&h->col, pcol, tb));
-    if (h->acc_mode == 0) TRY(upload(&h->cnt, pcnt, tb));
-    else TRY(upload(&h->wfx, pwfx, tb));
+    TRY(upload(&h->rowptr, H.rp, tb));
+    TRY(upload(&h->col, H.pcol, tb));
+    if (h->acc_mode == 0) TRY(upload(&h->cnt, H.pcnt, tb));
+    else TRY(upload(&h->wfx, H.pwfx, tb));
     const size_t nb = (size_t)batch * n;
     const size_t rs = h->f64 ? sizeof(double) : sizeof(float);
     TRY(dalloc((char**)&h->v, nb * rs, tb));
@@ -431,10 +327,8 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
     h->list_group = h->plan.group > 0 ? h->plan.group : h->B;
     h->n_groups = (h->B + h->list_group - 1) / h->list_group;
     TRY(install_plastic(h, pos));
-    // worst case: every neuron of every instance fires in the same step
-    int64_t chunks_all = 0;
-    for (int64_t i = 0; i < n; i++) chunks_all += (ip[i + 1] - ip[i] + CHUNK - 1) / CHUNK;
-    h->cap_g = std::max<int64_t>(1, chunks_all * h->list_group);
+    // worst case: every neuron of every instance of a group fires in the same step
+    h->cap_g = std::max<int64_t>(1, H.chunks_all * h->list_group);
     TRY(dalloc(&h->items, (size_t)h->R * h->n_groups * h->cap_g, tb));
     TRY(dalloc(&h->item_count, (size_t)h->R * h->n_groups, tb));
     TRY(dalloc(&h->reset_tick, (size_t)batch, tb));
@@ -579,14 +473,14 @@ extern "C" int fb_set_plastic(fb_brain* h, const int64_t* pos, int64_t count)
 {
     if (!h || (count > 0 && !pos)) return fail(FB_ERR_ARG, "NULL argument");
     CU(cudaSetDevice(h->device));
-    std::vector<int64_t> all = h->h_pos;
+    std::vector<int64_t> all = h->plastic.pos;
     for (int64_t k = 0; k < count; k++) {
         if (pos[k] < 0 || pos[k] >= h->nnz) return fail(FB_ERR_ARG, "plastic position %lld out of range", (long long)pos[k]);
         all.push_back(pos[k]);
     }
     std::sort(all.begin(), all.end());
     all.erase(std::unique(all.begin(), all.end()), all.end());
-    if (all.size() == h->h_pos.size()) return FB_OK;
+    if (all.size() == h->plastic.pos.size()) return FB_OK;
     CU(cudaDeviceSynchronize());
     int rc = install_plastic(h, all);
     if (rc) return rc;
