@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
+    ap.add_argument("--engine", default="auto", choices=["auto", "step", "persistent"])
+    ap.add_argument("--lanes", type=int, default=0, help="lanes per spike work item (8/16/32; 0 = default)")
     return ap.parse_args()
 
 
@@ -250,6 +252,7 @@ def run_ours(args, world, rank, local):
     fs = wl.frame_steps(DT)
     frames = args.warmup + args.steps
     gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=1000 + rank, plastic_pos=pos)
+    gb.set_schedule(args.engine, lanes=args.lanes)
     idx_in = np.r_[drive.inputs, drive.tonic]
     j = gb.slots(idx_in).cpu().numpy()
     assert np.array_equal(np.sort(j), np.arange(len(idx_in))), "inputs own the first ext slots"
