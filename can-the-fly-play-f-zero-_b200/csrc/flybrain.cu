@@ -20,6 +20,14 @@ namespace {
 
 thread_local std::string g_err;
 
+}  // namespace
+
+namespace fb {
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace fb
+
+namespace {
+
 int fail(int code, const char* fmt, ...)
 {
     char buf[512];

@@ -16,8 +16,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(ROOT, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libflybrain.so")
-SOURCES = ["flybrain.cu"]
-HEADERS = ["common.cuh", "engine.cuh", "persist.cuh"]
+SOURCES = ["flybrain.cu", "static_run.cu"]
+HEADERS = ["common.cuh", "engine.cuh", "persist.cuh", "host_prep.hpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

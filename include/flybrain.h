@@ -143,6 +143,36 @@ int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_
  * Synchronises `stream`. Returns FB_OK or the first raised FB_ERR_* code. */
 int fb_check(fb_brain* brain, void* stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Run without any allocation by the library. (This entry point has no counterpart in the
+ * reference: it serves callers that cannot allocate device memory at run time, e.g. a program
+ * whose GPU memory is owned entirely by another allocator's pool, a control loop that cannot take
+ * the device synchronisation a cudaMalloc/cudaFree implies, or a deployment that forbids run-time
+ * allocation after start-up.)
+ *
+ * One instance, every buffer caller-owned and on the device: the CSR exactly as the reference
+ * keeps it on the GPU (indptr int64 n+1, indices int32, weights float32 already x w_syn, like
+ * flyzero/gpu.py:157-159 with no plastic entries), the state v, g (float32 n) and ref (int8 n),
+ * optional ext inputs (ext_idx int32 n, p_ext and bias_ext float32 n_ext; ext_idx NULL = none),
+ * and counts (int32 n, overwritten). Poisson kicks use the counter hash with `seed`, `step_no`
+ * (first step) and tick t0 (first step), like fb_run. The result equals fb_run of an engine
+ * created with FB_FLAG_ACC_FIXED, bit for bit.
+ *
+ * Its only scratch, the synaptic input in flight, lives in an array compiled into the library:
+ * FB_STATIC_RING_ENTRIES int64 (8 MiB), present on every GPU that loads the library until the
+ * process exits. A network fits if n * (n_delay + 1) <= FB_STATIC_RING_ENTRIES; larger ones are
+ * rejected with FB_ERR_ARG. The array is shared by every call and keeps what the last call left:
+ * clear != 0 zeroes the in-flight input first (start of a simulation); clear == 0 continues the
+ * previous call's simulation. Calls that overlap on the GPU (other streams, other threads) race
+ * on the array. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. No cudaMalloc, cudaFree
+ * or allocating library routine is called. */
+#define FB_STATIC_RING_ENTRIES 1048576
+int fb_run_static(const fb_params* params, int64_t n, const int64_t* indptr, const int32_t* indices,
+                  const float* weights, float* v, float* g, int8_t* ref, const int32_t* ext_idx,
+                  const float* p_ext, const float* bias_ext, uint32_t seed, uint32_t step_no, int64_t t0,
+                  int32_t steps, int32_t clear, int32_t* counts, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
