@@ -158,6 +158,8 @@ struct fb_brain {
     int32_t n_groups = 1;
     unsigned int* bar = nullptr;  // persistent grid-barrier counter
     int32_t* abort_flag = nullptr;
+    int2* ext_tab = nullptr;      // persistent engine: input pairs of each CTA
+    int32_t* ext_off = nullptr;
     int64_t* reset_tick = nullptr;
     int64_t* stop_tick = nullptr;
     uint8_t* fly_mask = nullptr;
@@ -203,7 +205,8 @@ int free_all(fb_brain* h)
 {
     void* ptrs[] = {h->rowptr, h->col, h->cnt, h->wfx, h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->pw, h->w0,
                     h->v, h->g, h->ref, h->ext_idx, h->p_ext, h->bias_ext, h->acc[0], h->acc[1], h->pring,
-                    h->items, h->item_count, h->reset_tick, h->stop_tick, h->fly_mask, h->bar, h->abort_flag};
+                    h->items, h->item_count, h->reset_tick, h->stop_tick, h->fly_mask, h->bar, h->abort_flag,
+                    h->ext_tab, h->ext_off};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : h->graveyard) cudaFree(p);
@@ -250,6 +253,34 @@ int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
     h->n_ppost = P.n_ppost;
     h->plastic = std::move(P);
     return FB_OK;
+}
+
+// Per-CTA table of the persistent engine's input pairs (pairs whose neuron has an ext slot):
+// entry {local pair | instance-in-group << 18, ext slot}, grouped by CTA. Rebuilt when the ext
+// map changes; the same table serves every group (pairs are numbered within a group).
+int build_ext_table(fb_brain* h)
+{
+    const PersistPlan& P = h->plan;
+    if (P.group == 0) return FB_OK;
+    std::vector<int32_t> off(P.ctas + 1, 0);
+    std::vector<int2> tab;
+    const int64_t np = h->n_pad, total = (int64_t)P.group * np;
+    for (int32_t c = 0; c < P.ctas; c++) {
+        off[c] = (int32_t)tab.size();
+        const int64_t lo = (int64_t)c * P.per, hi = std::min(lo + P.per, total);
+        for (int64_t p = lo; p < hi; p++) {
+            const int64_t bl = p / np, i = p - bl * np;
+            if (i < h->n && h->h_ext_idx[i] >= 0) tab.push_back(make_int2((int32_t)((p - lo) | (bl << 18)), h->h_ext_idx[i]));
+        }
+    }
+    off[P.ctas] = (int32_t)tab.size();
+    if (h->ext_tab) h->graveyard.push_back(h->ext_tab);
+    if (h->ext_off) h->graveyard.push_back(h->ext_off);
+    h->ext_tab = nullptr;
+    h->ext_off = nullptr;
+    int rc = upload(&h->ext_tab, tab, &h->bytes);
+    if (rc) return rc;
+    return upload(&h->ext_off, off, &h->bytes);
 }
 
 int dispatch_step(fb_brain* h, const StepArgs& A, bool raster, bool record, cudaStream_t st);
@@ -335,6 +366,7 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
     h->list_group = h->plan.group > 0 ? h->plan.group : h->B;
     h->n_groups = (h->B + h->list_group - 1) / h->list_group;
     TRY(install_plastic(h, pos));
+    TRY(build_ext_table(h));
     // worst case: every neuron of every instance of a group fires in the same step
     h->cap_g = std::max<int64_t>(1, H.chunks_all * h->list_group);
     TRY(dalloc(&h->items, (size_t)h->R * h->n_groups * h->cap_g, tb));
@@ -435,6 +467,8 @@ extern "C" int fb_set_ext(fb_brain* h, const int64_t* idx, int64_t count)
     h->p_ext = np_;
     h->bias_ext = nb_;
     h->n_ext = now;
+    rc = build_ext_table(h);
+    if (rc) return rc;
     CU(cudaDeviceSynchronize());
     return FB_OK;
 }
@@ -600,7 +634,7 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         PersistArgs P{};
         P.t0 = h->t; P.step0 = h->step_no; P.steps = steps; P.kicks = kicks; P.words = words;
         P.counts = counts_out; P.step_counts = step_counts; P.step_digest = step_digest;
-        P.bar = h->bar; P.abort_flag = h->abort_flag;
+        P.bar = h->bar; P.abort_flag = h->abort_flag; P.ext_tab = h->ext_tab; P.ext_off = h->ext_off;
         CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
         int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
                                    record, h->lanes, st);

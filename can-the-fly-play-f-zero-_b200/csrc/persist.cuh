@@ -17,9 +17,9 @@
 
 namespace fb {
 
-constexpr int PT = 512;                 // threads per CTA
-constexpr int STAGE_BYTES = 16384;      // one TMA stage
-constexpr int NSTAGE = 3;
+constexpr int PT = 1024;                // threads per CTA
+constexpr int ZERO_PAGE = 4096;         // shared-memory zeros, the source of the clearing bulk stores
+constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulator slice
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
 
 struct PersistPlan {
@@ -42,6 +42,8 @@ struct PersistArgs {
     uint64_t* step_digest;
     unsigned int* bar;        // zeroed before the launch
     int32_t* abort_flag;      // zeroed before the launch
+    const int2* ext_tab;      // per CTA: input pairs {k | instance << 18, ext slot}
+    const int32_t* ext_off;   // (ctas + 1) offsets into ext_tab
 };
 
 // ---- PTX helpers: mbarrier, TMA 1-D bulk copy, proxy fences, acquire load --------------------
@@ -127,150 +129,220 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
     return true;
 }
 
+// Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
+struct PersistSmem {
+    int64_t mbar, zero, acc, v, g, kbits, ref, active, total;
+    __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
+    {
+        const int64_t words = (per + PT - 1) / PT * PT / 32;
+        mbar = 0;
+        zero = 128;
+        acc = zero + ZERO_PAGE;
+        v = acc + per * acc_bytes;
+        g = v + per * 4;
+        kbits = g + per * 4;
+        ref = kbits + words * 4;
+        active = (ref + per + 15) / 16 * 16;
+        total = active + 64;
+    }
+};
+
+// Append this lane's work items to the list of group q (all lanes of the warp belong to q).
+__device__ __forceinline__ void warp_append_q(const DevState& S, int64_t slot, int32_t q, int nch, int32_t i, int32_t b)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int incl = nch;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
+    int base = 0;
+    if (lane == 31) base = atomicAdd(count_of(S, slot, q), total);
+    base = __shfl_sync(FULL, base, 31);
+    int2* list = list_of(S, slot, q);
+    const int64_t start = (int64_t)base + incl - nch;
+    for (int c = 0; c < nch; c++) {
+        const int64_t p = start + c;
+        if (p < S.cap_g) list[p] = make_int2(i, (b << CHUNK_BITS) | c);
+        else atomicExch(S.err, 1);
+    }
+}
+
+// bulk store shared -> global (16-byte aligned, size a multiple of 16), tracked by bulk groups
+__device__ __forceinline__ void tma_store_1d(void* dst_gmem, const void* src_smem, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst_gmem), "r"(smem_u32(src_smem)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
 template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD, int LANES>
 __global__ void __launch_bounds__(PT, 1)
     k_persist(const DevNet N, const DevState S, const PersistArgs A, int32_t b0, int32_t G, int32_t q, int64_t per)
 {
     extern __shared__ __align__(128) uint8_t smem[];
-    constexpr int SP = STAGE_BYTES / (int)sizeof(AccT);    // pairs per stage (multiple of PT)
-    AccT* stage = reinterpret_cast<AccT*>(smem);
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + NSTAGE * STAGE_BYTES);
-    float* sv = reinterpret_cast<float*>(mbar + NSTAGE);
-    float* sg = sv + per;
-    uint8_t* sr = reinterpret_cast<uint8_t*>(sg + per);    // bits 0-5 refractory, 6 plastic target, 7 ext
-    uint8_t* s_active = sr + per;                          // G flags
+    const PersistSmem lay(per, (int)sizeof(AccT));
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + lay.mbar);
+    const uint8_t* zero = smem + lay.zero;
+    AccT* sacc = reinterpret_cast<AccT*>(smem + lay.acc);
+    float* sv = reinterpret_cast<float*>(smem + lay.v);
+    float* sg = reinterpret_cast<float*>(smem + lay.g);
+    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + lay.kbits);   // Poisson kicks of this step
+    uint8_t* sr = smem + lay.ref;        // bits 0-5 refractory, 6 plastic target, 7 nonzero bias
+    uint8_t* s_active = smem + lay.active;
     const Lif<float>& L = N.L32;
     const int tid = threadIdx.x;
+    const int lane = tid & 31;
     const int64_t n = N.n, np = N.n_pad;
     const int64_t lo = (int64_t)blockIdx.x * per;
-    const int64_t cnt = max((int64_t)0, min(per, (int64_t)G * np - lo));
+    const int32_t cnt = (int32_t)max((int64_t)0, min(per, (int64_t)G * np - lo));
     const int64_t acc_base = (int64_t)b0 * np + lo;       // accumulator index of local pair 0
     float* V = reinterpret_cast<float*>(S.v);
     float* Gs = reinterpret_cast<float*>(S.g);
+    const int32_t e0 = A.ext_off[blockIdx.x], e1 = A.ext_off[blockIdx.x + 1];
+    const int32_t nwords = (int32_t)((per + PT - 1) / PT * PT / 32);
 
     // ---- load this CTA's state into shared memory ------------------------------------------
-    for (int64_t k = tid; k < cnt; k += PT) {
+    for (int32_t k = tid; k < cnt; k += PT) {
         const int64_t lp = lo + k;
         const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
+        uint8_t f = 0;
         if (i < n) {
             const int64_t gp = (int64_t)(b0 + bl) * n + i;
             sv[k] = V[gp];
             sg[k] = Gs[gp];
-            uint8_t f = (uint8_t)S.ref[gp];
-            if (S.ext_idx[i] >= 0) f |= 0x80;
+            f = (uint8_t)S.ref[gp];
             if (PLASTIC && N.ppost_of[i] >= 0) f |= 0x40;
-            sr[k] = f;
         }
+        sr[k] = f;
     }
+    for (int32_t w = tid; w < nwords; w += PT) kbits[w] = 0u;
+    for (int32_t z = tid; z < ZERO_PAGE / 4; z += PT) reinterpret_cast<uint32_t*>(smem + lay.zero)[z] = 0u;
+    fence_proxy_async_shared();                                  // zero page visible to bulk copies
     if (tid == 0) {
-        for (int s = 0; s < NSTAGE; s++) mbar_init(&mbar[s], 1);
+        mbar_init(mbar, 1);
         fence_mbar_init();
     }
     __syncthreads();
+    for (int32_t e = e0 + tid; e < e1; e += PT) {               // bias is constant during a launch
+        const int2 en = __ldg(A.ext_tab + e);
+        const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
+        if (bl < G && S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + en.y] != 0.0f) sr[k] |= 0x80;
+    }
+    __syncthreads();
 
-    const int64_t nchunks = (cnt + SP - 1) / SP;
-    uint32_t phase_bits = 0;          // parity of each stage's next completion
     unsigned int barriers = 0;
     int32_t* err = S.err;
     const int32_t nthreads_grid = gridDim.x * PT;
     const int64_t gtid = (int64_t)blockIdx.x * PT + tid;
-    const int32_t words = A.words;
+    const uint32_t acc_bytes = (uint32_t)cnt * (uint32_t)sizeof(AccT);
+    const int32_t i0 = (int32_t)((lo + tid) % np), bl0 = (int32_t)((lo + tid) / np);
 
     for (int32_t s = 0; s < A.steps; s++) {
         const int64_t t = A.t0 + s;
         const uint32_t step_no = A.step0 + (uint32_t)s;
+        const AccT* acc = reinterpret_cast<const AccT*>((t & 1) ? S.acc1 : S.acc0);
+        // (1) the accumulator slice of this step -> shared memory, one bulk load
+        if (tid == 0 && cnt > 0) {
+            fence_proxy_async_global();
+            mbar_expect_tx(mbar, acc_bytes);
+            for (uint32_t off = 0; off < acc_bytes; off += LOAD_PIECE)
+                tma_load_1d(reinterpret_cast<uint8_t*>(sacc) + off,
+                            reinterpret_cast<const uint8_t*>(acc + acc_base) + off, min((uint32_t)LOAD_PIECE, acc_bytes - off),
+                            mbar);
+        }
         if (tid < G) s_active[tid] = t < S.stop_tick[b0 + tid];
         if (blockIdx.x == 0 && tid == 0) *count_of(S, pos_mod(t - N.n_delay, N.R), q) = 0;
         __syncthreads();
-        const AccT* acc = reinterpret_cast<const AccT*>((t & 1) ? S.acc1 : S.acc0);
-        AccT* accw = const_cast<AccT*>(acc);
-        const int64_t slot = pos_mod(t, N.R);
-
-        // ---- U: advance every owned pair -----------------------------------------------------
-        if (tid == 0) {
-            fence_proxy_async_global();
-            for (int64_t c = 0; c < min((int64_t)NSTAGE, nchunks); c++) {
-                const uint32_t bytes = (uint32_t)(min((int64_t)SP, cnt - c * SP) * (int64_t)sizeof(AccT));
-                mbar_expect_tx(&mbar[c], bytes);
-                tma_load_1d(stage + c * SP, acc + acc_base + c * SP, bytes, &mbar[c]);
+        // (2) Poisson kicks of the input pairs (overlaps the load)
+        for (int32_t e = e0 + tid; e < e1; e += PT) {
+            const int2 en = __ldg(A.ext_tab + e);
+            const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
+            if (bl >= G || !s_active[bl]) continue;
+            const int32_t b = b0 + bl;
+            const int32_t i = (int32_t)(lo + k - (int64_t)bl * np);
+            if (kick_of<RASTER>(S, A.kicks, A.words, N.B, s, b, en.y, (uint32_t)((int64_t)b * n + i), step_no))
+                atomicOr(kbits + (k >> 5), 1u << (k & 31));
+        }
+        __syncthreads();
+        bool stop = false;
+        if (cnt > 0) {
+            stop = !stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
+            // (3) the slice is in shared memory: clear it in global memory with bulk stores
+            if (tid == 0 && !stop) {
+                AccT* accw = const_cast<AccT*>(acc) + acc_base;
+                for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
+                    tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
+                bulk_commit();
             }
         }
-        int64_t lp = lo + tid;
-        int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
-        bool stop = false;
-        for (int64_t c = 0; c < nchunks; c++) {
-            const int st = (int)(c % NSTAGE);
-            if (!stage_wait(&mbar[st], (phase_bits >> st) & 1u, A, err, s + 1)) { stop = true; }
-            phase_bits ^= 1u << st;
-            const AccT* sa = stage + st * SP;
-#pragma unroll 2
-            for (int m = 0; m < SP / PT; m++) {
-                const int64_t k = c * SP + m * PT + tid;       // local pair
-                int nch = 0;
-                if (k < cnt && i < n && s_active[bl] && !stop) {
-                    const int32_t b = b0 + bl;
-                    const AccT x = sa[m * PT + tid];
-                    if (x != 0) accw[acc_base + k] = 0;
-                    float buf = acc_to_real<float>(x, L.w_syn);
-                    const uint8_t f = sr[k];
-                    if (PLASTIC && (f & 0x40)) buf = add_rn(buf, take_plastic<float>(N, S, t, b, i));
-                    float v = sv[k], g = sg[k];
-                    int r = f & 0x3f;
-                    float bias = 0.0f;
-                    bool kicked = false;
-                    const bool ext = (f & 0x80) != 0;
-                    const uint32_t tidh = (uint32_t)((int64_t)b * n + i);
-                    if (ext) {
-                        const int32_t j = S.ext_idx[i];
-                        bias = S.bias_ext[(int64_t)b * S.n_ext + j];
-                        kicked = kick_of<RASTER>(S, A.kicks, words, N.B, s, b, j, tidh, step_no);
-                    }
-                    const bool spk = lif_step<float>(v, g, r, buf, ext, bias, kicked, L, N.n_ref, N.contract != 0);
-                    sv[k] = v;
-                    sg[k] = g;
-                    sr[k] = (uint8_t)((f & 0xc0) | r);
-                    if (spk) {
-                        A.counts[(int64_t)b * n + i] += 1;
-                        const int64_t len = N.rowptr[i + 1] - N.rowptr[i];
-                        nch = (int)((len + CHUNK - 1) / CHUNK);
-                        if (PLASTIC) push_plastic_row(N, S, t, b, i);
-                        if (RECORD) {
-                            if (A.step_counts) atomicAdd(A.step_counts + (int64_t)s * N.B + b, 1);
-                            if (A.step_digest)
-                                atomicAdd(reinterpret_cast<unsigned long long*>(A.step_digest + (int64_t)s * N.B + b),
-                                          (unsigned long long)spike_tag((uint64_t)i));
-                        }
+        stop = __syncthreads_or(stop) != 0;
+        if (stop) break;
+        // (4) advance every owned pair
+        const int64_t slot = pos_mod(t, N.R);
+        int32_t i = i0, bl = bl0;
+        for (int32_t kb = 0; kb < cnt; kb += PT) {
+            const int32_t k = kb + tid;
+            const uint32_t kw = kbits[k >> 5];
+            __syncwarp();
+            if (lane == 0) kbits[k >> 5] = 0u;
+            int nch = 0;
+            if (k < cnt && i < n && s_active[bl]) {
+                const int32_t b = b0 + bl;
+                float buf = acc_to_real<float>(sacc[k], L.w_syn);
+                const uint32_t f = sr[k];
+                if (PLASTIC && (f & 0x40)) buf = add_rn(buf, take_plastic<float>(N, S, t, b, i));
+                float v = sv[k], g = sg[k];
+                int r = (int)(f & 0x3f);
+                const bool hb = (f & 0x80) != 0;
+                const float bias = hb ? S.bias_ext[(int64_t)b * S.n_ext + S.ext_idx[i]] : 0.0f;
+                const bool spk = lif_step<float>(v, g, r, buf, hb, bias, (kw >> lane) & 1u, L, N.n_ref, N.contract != 0);
+                sv[k] = v;
+                sg[k] = g;
+                sr[k] = (uint8_t)((f & 0xc0) | (uint32_t)r);
+                if (spk) {
+                    A.counts[(int64_t)b * n + i] += 1;
+                    const int64_t len = N.rowptr[i + 1] - N.rowptr[i];
+                    nch = (int)((len + CHUNK - 1) / CHUNK);
+                    if (PLASTIC) push_plastic_row(N, S, t, b, i);
+                    if (RECORD) {
+                        if (A.step_counts) atomicAdd(A.step_counts + (int64_t)s * N.B + b, 1);
+                        if (A.step_digest)
+                            atomicAdd(reinterpret_cast<unsigned long long*>(A.step_digest + (int64_t)s * N.B + b),
+                                      (unsigned long long)spike_tag((uint64_t)i));
                     }
                 }
-                warp_append(S, slot, nch, i, b0 + bl);
-                i += PT;
-                while (i >= np) { i -= (int32_t)np; bl++; }
             }
-            stop = __syncthreads_or(stop) != 0;                // stage st consumed by every thread
-            if (tid == 0 && c + NSTAGE < nchunks && !stop) {
-                fence_proxy_async_shared();
-                const int64_t cn = c + NSTAGE;
-                const uint32_t bytes = (uint32_t)(min((int64_t)SP, cnt - cn * SP) * (int64_t)sizeof(AccT));
-                mbar_expect_tx(&mbar[st], bytes);
-                tma_load_1d(stage + st * SP, acc + acc_base + cn * SP, bytes, &mbar[st]);
-            }
+            if (__ballot_sync(0xffffffffu, nch > 0)) warp_append_q(S, slot, q, nch, i, b0 + bl);
+            i += PT;
+            while (i >= np) { i -= (int32_t)np; bl++; }
         }
-        if (stop) break;
+        fence_proxy_async_shared();          // this step's reads of the slice before the next bulk load
 
-        // ---- P: scatter the spikes that arrive at t+1 ----------------------------------------
+        // (5) scatter the spikes that arrive at t+1 into the other accumulator
         if (N.n_delay == 1) {
             barriers++;
             if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) break;
         }
         AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
         push_list<AccT, LANES>(N, S, t, q, acc_next, gtid, nthreads_grid);
+        if (tid == 0 && cnt > 0) {
+            bulk_wait_all();                      // the cleared slice is written before anyone pushes into it
+            fence_proxy_async_global();
+        }
         barriers++;
         if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) break;
     }
+    if (tid == 0) bulk_wait_all();
 
     // ---- write the state back ------------------------------------------------------------------
     __syncthreads();
-    for (int64_t k = tid; k < cnt; k += PT) {
+    for (int32_t k = tid; k < cnt; k += PT) {
         const int64_t lp2 = lo + k;
         const int32_t bl2 = (int32_t)(lp2 / np), i2 = (int32_t)(lp2 - (int64_t)bl2 * np);
         if (i2 < n) {
@@ -291,25 +363,29 @@ inline PersistPlan plan_persistent(int64_t n, int64_t n_pad, int32_t B, bool f64
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (smem_optin <= 0) smem_optin = 232448;
-    const int64_t fixed = NSTAGE * STAGE_BYTES + NSTAGE * 8 + 64 /* group flags */ + 256;
-    const int64_t per_max = ((smem_optin - fixed) / 9) / 16 * 16;
+    int64_t per_max = 0;
+    for (int64_t lo = 16, hi = (int64_t)1 << 18; lo <= hi;) {     // largest `per` whose layout fits
+        const int64_t mid = (lo + hi) / 2 / 16 * 16;
+        if (mid < 16) break;
+        if (PersistSmem(mid, acc_bytes).total <= smem_optin) { per_max = mid; lo = mid + 16; }
+        else hi = mid - 16;
+    }
     if (per_max <= 0) return P;
     const int ctas = sm_count;
-    int64_t gmax = (int64_t)ctas * per_max / n_pad;
-    gmax = std::min<int64_t>(gmax, 64);
+    int64_t gmax = std::min<int64_t>((int64_t)ctas * per_max / n_pad, 63);
     if (gmax < 1) return P;
     const int32_t n_groups = (int32_t)((B + gmax - 1) / gmax);
     const int32_t G = (B + n_groups - 1) / n_groups;
     int64_t per = ((int64_t)G * n_pad + ctas - 1) / ctas;
     per = (per + 15) / 16 * 16;
-    if (per > per_max) return P;
+    if (per > per_max || per >= ((int64_t)1 << 18)) return P;
     P.group = G;
     P.n_groups = n_groups;
     P.ctas = ctas;
     P.per = per;
-    P.smem = (size_t)(fixed + per * 9);
+    P.smem = (size_t)PersistSmem(per, acc_bytes).total;
     P.launches_per_run = n_groups;
-    (void)n; (void)acc_bytes;
+    (void)n;
     return P;
 }
 
