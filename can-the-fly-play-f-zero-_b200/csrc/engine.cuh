@@ -97,9 +97,19 @@ __device__ __forceinline__ int32_t* count_of(const DevState& S, int64_t slot, in
     return S.item_count + (int64_t)slot * S.n_groups + q;
 }
 
+// A work item: up to CHUNK consecutive entries of a spiking row, {first entry in the padded CSR,
+// (instance << CHUNK_BITS) | number of entries}.
+__device__ __forceinline__ int2 make_item(const DevNet& N, int32_t i, int32_t b, int c)
+{
+    const int64_t r0 = N.rowptr[i], r1 = N.rowptr[i + 1];
+    const int64_t k0 = r0 + (int64_t)c * CHUNK;
+    return make_int2((int32_t)k0, (b << CHUNK_BITS) | (int32_t)min((int64_t)CHUNK, r1 - k0));
+}
+
 // Append `nch` work items (this lane's spike: chunks 0..nch-1 of row i of instance b) to the list
 // of the lane's instance group; one atomic per warp and group (the ballot/shuffle compaction).
-__device__ __forceinline__ void warp_append(const DevState& S, int64_t slot, int nch, int32_t i, int32_t b)
+__device__ __forceinline__ void warp_append(const DevNet& N, const DevState& S, int64_t slot, int nch, int32_t i,
+                                            int32_t b)
 {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -124,7 +134,7 @@ __device__ __forceinline__ void warp_append(const DevState& S, int64_t slot, int
             const int64_t start = (int64_t)base + incl - nch;
             for (int c = 0; c < nch; c++) {
                 const int64_t p = start + c;
-                if (p < S.cap_g) list[p] = make_int2(i, (b << CHUNK_BITS) | c);
+                if (p < S.cap_g) list[p] = make_item(N, i, b, c);
                 else atomicExch(S.err, 1);
             }
         }
@@ -229,7 +239,7 @@ __global__ void __launch_bounds__(256) k_update(const DevNet N, const DevState S
                 }
             }
         }
-        warp_append(S, slot, nch, i, b);
+        warp_append(N, S, slot, nch, i, b);
     }
 }
 
@@ -280,11 +290,9 @@ __device__ __forceinline__ void red_add(int64_t* p, int64_t x)
 
 // Scatter one work item (<= CHUNK entries of a spiking row) with LANES lanes, 8 entries a lane.
 template <typename AccT, int LANES>
-__device__ __forceinline__ void push_item(const DevNet& N, AccT* acc_b, int32_t i, int32_t c, int lane)
+__device__ __forceinline__ void push_item(const DevNet& N, AccT* acc_b, int64_t k0, int32_t len, int lane)
 {
-    const int64_t r1 = N.rowptr[i + 1];
-    const int64_t k0 = N.rowptr[i] + (int64_t)c * CHUNK;
-    const int64_t k1 = min(k0 + (int64_t)CHUNK, r1);
+    const int64_t k1 = k0 + len;
     for (int64_t k = k0 + (int64_t)lane * 8; k < k1; k += LANES * 8) {
         Edges8<AccT> e;
         e.load(N, k);
@@ -311,7 +319,8 @@ __device__ __forceinline__ void push_list(const DevNet& N, const DevState& S, in
         const int2 item = __ldcg(list + it);
         const int32_t b = item.y >> CHUNK_BITS;
         if (s < S.reset_tick[b] || t + 1 >= S.stop_tick[b]) continue;
-        push_item<AccT, LANES>(N, acc_next + (int64_t)b * N.n_pad, item.x, item.y & ((1 << CHUNK_BITS) - 1), lane);
+        push_item<AccT, LANES>(N, acc_next + (int64_t)b * N.n_pad, (int64_t)(uint32_t)item.x,
+                               item.y & ((1 << CHUNK_BITS) - 1), lane);
     }
 }
 

@@ -173,7 +173,7 @@ struct fb_brain {
     // schedule
     int engine = FB_ENGINE_AUTO;
     int prop = FB_PROP_PUSH;
-    int lanes = 32;
+    int lanes = 8;
     int sm_count = 148;
     PersistPlan plan{};
 

@@ -131,10 +131,10 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
 
 // Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
 struct PersistSmem {
-    int64_t mbar, zero, acc, v, g, kbits, ref, active, total;
+    int64_t mbar, zero, acc, v, g, kbits, ref, misc, total;
     __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
     {
-        const int64_t words = (per + PT - 1) / PT * PT / 32;
+        const int64_t words = (per + 4 * PT) / 32 + 1;
         mbar = 0;
         zero = 128;
         acc = zero + ZERO_PAGE;
@@ -142,33 +142,28 @@ struct PersistSmem {
         g = v + per * 4;
         kbits = g + per * 4;
         ref = kbits + words * 4;
-        active = (ref + per + 15) / 16 * 16;
-        total = active + 64;
+        misc = (ref + per + 15) / 16 * 16;   // 64 active flags + 4 counters
+        total = misc + 64 + 16;
     }
 };
 
-// Append this lane's work items to the list of group q (all lanes of the warp belong to q).
-__device__ __forceinline__ void warp_append_q(const DevState& S, int64_t slot, int32_t q, int nch, int32_t i, int32_t b)
+constexpr int P_WARPS = 4;                     // warps of a CTA that scatter spikes (P) ...
+constexpr int U_THREADS = PT - 32 * P_WARPS;   // ... while the other 896 threads advance neurons (U)
+
+__device__ __forceinline__ void u_sync() { asm volatile("bar.sync 1, %0;" ::"n"(U_THREADS) : "memory"); }
+// barrier of the U threads that also ORs a predicate over them (so every U thread sees the same value)
+__device__ __forceinline__ bool u_sync_or(bool pred)
 {
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    int incl = nch;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const int total = __shfl_sync(FULL, incl, 31);
-    int base = 0;
-    if (lane == 31) base = atomicAdd(count_of(S, slot, q), total);
-    base = __shfl_sync(FULL, base, 31);
-    int2* list = list_of(S, slot, q);
-    const int64_t start = (int64_t)base + incl - nch;
-    for (int c = 0; c < nch; c++) {
-        const int64_t p = start + c;
-        if (p < S.cap_g) list[p] = make_int2(i, (b << CHUNK_BITS) | c);
-        else atomicExch(S.err, 1);
-    }
+    uint32_t out;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred p, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(out)
+        : "r"((uint32_t)pred), "n"(U_THREADS)
+        : "memory");
+    return out != 0;
 }
 
 // bulk store shared -> global (16-byte aligned, size a multiple of 16), tracked by bulk groups
@@ -181,6 +176,18 @@ __device__ __forceinline__ void tma_store_1d(void* dst_gmem, const void* src_sme
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
+// four consecutive accumulator entries from shared memory (16-byte aligned)
+__device__ __forceinline__ void load4(const int32_t* p, int32_t (&x)[4])
+{
+    const int4 v = *reinterpret_cast<const int4*>(p);
+    x[0] = v.x; x[1] = v.y; x[2] = v.z; x[3] = v.w;
+}
+__device__ __forceinline__ void load4(const int64_t* p, int64_t (&x)[4])
+{
+    const longlong2 a = reinterpret_cast<const longlong2*>(p)[0], b = reinterpret_cast<const longlong2*>(p)[1];
+    x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
+}
+
 template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD, int LANES>
 __global__ void __launch_bounds__(PT, 1)
     k_persist(const DevNet N, const DevState S, const PersistArgs A, int32_t b0, int32_t G, int32_t q, int64_t per)
@@ -192,20 +199,23 @@ __global__ void __launch_bounds__(PT, 1)
     AccT* sacc = reinterpret_cast<AccT*>(smem + lay.acc);
     float* sv = reinterpret_cast<float*>(smem + lay.v);
     float* sg = reinterpret_cast<float*>(smem + lay.g);
-    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + lay.kbits);   // Poisson kicks of this step
-    uint8_t* sr = smem + lay.ref;        // bits 0-5 refractory, 6 plastic target, 7 nonzero bias
-    uint8_t* s_active = smem + lay.active;
+    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + lay.kbits);  // kicks before U, spikes after
+    uint8_t* sr = smem + lay.ref;            // bits 0-5 refractory, 6 plastic target, 7 nonzero bias
+    uint8_t* s_active = smem + lay.misc;
+    int32_t* s_cnt = reinterpret_cast<int32_t*>(smem + lay.misc + 64);   // total, cursor, base
     const Lif<float>& L = N.L32;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const int64_t n = N.n, np = N.n_pad;
+    const bool u_warp = tid < U_THREADS;
+    const int32_t n = (int32_t)N.n, np = (int32_t)N.n_pad;
     const int64_t lo = (int64_t)blockIdx.x * per;
     const int32_t cnt = (int32_t)max((int64_t)0, min(per, (int64_t)G * np - lo));
     const int64_t acc_base = (int64_t)b0 * np + lo;       // accumulator index of local pair 0
     float* V = reinterpret_cast<float*>(S.v);
     float* Gs = reinterpret_cast<float*>(S.g);
     const int32_t e0 = A.ext_off[blockIdx.x], e1 = A.ext_off[blockIdx.x + 1];
-    const int32_t nwords = (int32_t)((per + PT - 1) / PT * PT / 32);
+    const int32_t nwords = (int32_t)((per + 4 * PT) / 32 + 1);
+    const int32_t used_words = (cnt + 31) / 32;
 
     // ---- load this CTA's state into shared memory ------------------------------------------
     for (int32_t k = tid; k < cnt; k += PT) {
@@ -238,16 +248,17 @@ __global__ void __launch_bounds__(PT, 1)
 
     unsigned int barriers = 0;
     int32_t* err = S.err;
-    const int32_t nthreads_grid = gridDim.x * PT;
-    const int64_t gtid = (int64_t)blockIdx.x * PT + tid;
     const uint32_t acc_bytes = (uint32_t)cnt * (uint32_t)sizeof(AccT);
-    const int32_t i0 = (int32_t)((lo + tid) % np), bl0 = (int32_t)((lo + tid) / np);
+    const int32_t i0 = (int32_t)((lo + 4 * tid) % np), bl0 = (int32_t)((lo + 4 * tid) / np);
+    const int64_t p_tid = (int64_t)blockIdx.x * (PT - U_THREADS) + (tid - U_THREADS);
+    const int64_t p_threads = (int64_t)gridDim.x * (PT - U_THREADS);
 
     for (int32_t s = 0; s < A.steps; s++) {
         const int64_t t = A.t0 + s;
         const uint32_t step_no = A.step0 + (uint32_t)s;
         const AccT* acc = reinterpret_cast<const AccT*>((t & 1) ? S.acc1 : S.acc0);
-        // (1) the accumulator slice of this step -> shared memory, one bulk load
+        const int64_t slot = pos_mod(t, N.R);
+        // the accumulator slice of this step -> shared memory, one bulk load
         if (tid == 0 && cnt > 0) {
             fence_proxy_async_global();
             mbar_expect_tx(mbar, acc_bytes);
@@ -257,58 +268,91 @@ __global__ void __launch_bounds__(PT, 1)
                             mbar);
         }
         if (tid < G) s_active[tid] = t < S.stop_tick[b0 + tid];
-        if (blockIdx.x == 0 && tid == 0) *count_of(S, pos_mod(t - N.n_delay, N.R), q) = 0;
+        if (tid == 32) s_cnt[0] = s_cnt[1] = 0;
+        if (blockIdx.x == 0 && tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q) = 0;
         __syncthreads();
-        // (2) Poisson kicks of the input pairs (overlaps the load)
-        for (int32_t e = e0 + tid; e < e1; e += PT) {
-            const int2 en = __ldg(A.ext_tab + e);
-            const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
-            if (bl >= G || !s_active[bl]) continue;
-            const int32_t b = b0 + bl;
-            const int32_t i = (int32_t)(lo + k - (int64_t)bl * np);
-            if (kick_of<RASTER>(S, A.kicks, A.words, N.B, s, b, en.y, (uint32_t)((int64_t)b * n + i), step_no))
-                atomicOr(kbits + (k >> 5), 1u << (k & 31));
-        }
-        __syncthreads();
-        bool stop = false;
-        if (cnt > 0) {
-            stop = !stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
-            // (3) the slice is in shared memory: clear it in global memory with bulk stores
-            if (tid == 0 && !stop) {
-                AccT* accw = const_cast<AccT*>(acc) + acc_base;
-                for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
-                    tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
-                bulk_commit();
-            }
-        }
-        stop = __syncthreads_or(stop) != 0;
-        if (stop) break;
-        // (4) advance every owned pair
-        const int64_t slot = pos_mod(t, N.R);
-        int32_t i = i0, bl = bl0;
-        for (int32_t kb = 0; kb < cnt; kb += PT) {
-            const int32_t k = kb + tid;
-            const uint32_t kw = kbits[k >> 5];
-            __syncwarp();
-            if (lane == 0) kbits[k >> 5] = 0u;
-            int nch = 0;
-            if (k < cnt && i < n && s_active[bl]) {
+        if (u_warp) {
+            // ---- U1: Poisson kicks of the input pairs into the bitmap (overlaps the load) ----------
+            for (int32_t e = e0 + tid; e < e1; e += U_THREADS) {
+                const int2 en = __ldg(A.ext_tab + e);
+                const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
+                if (bl >= G || !s_active[bl]) continue;
                 const int32_t b = b0 + bl;
-                float buf = acc_to_real<float>(sacc[k], L.w_syn);
-                const uint32_t f = sr[k];
-                if (PLASTIC && (f & 0x40)) buf = add_rn(buf, take_plastic<float>(N, S, t, b, i));
-                float v = sv[k], g = sg[k];
-                int r = (int)(f & 0x3f);
-                const bool hb = (f & 0x80) != 0;
-                const float bias = hb ? S.bias_ext[(int64_t)b * S.n_ext + S.ext_idx[i]] : 0.0f;
-                const bool spk = lif_step<float>(v, g, r, buf, hb, bias, (kw >> lane) & 1u, L, N.n_ref, N.contract != 0);
-                sv[k] = v;
-                sg[k] = g;
-                sr[k] = (uint8_t)((f & 0xc0) | (uint32_t)r);
-                if (spk) {
+                const int32_t i = (int32_t)(lo + k - (int64_t)bl * np);
+                if (kick_of<RASTER>(S, A.kicks, A.words, N.B, s, b, en.y, (uint32_t)((int64_t)b * n + i), step_no))
+                    atomicOr(kbits + (k >> 5), 1u << (k & 31));
+            }
+            u_sync();
+            bool ok = true;
+            if (cnt > 0 && tid == 0) ok = stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
+            ok = !u_sync_or(!ok);        // one thread waited; every U thread agrees on the outcome
+            if (cnt > 0 && ok) (void)mbar_try_wait(mbar, (uint32_t)(s & 1));   // completed: acquire only
+            if (cnt > 0) {
+                if (tid == 0 && ok) {    // the slice is in shared memory: clear it in global memory
+                    AccT* accw = const_cast<AccT*>(acc) + acc_base;
+                    for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
+                        tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
+                    bulk_commit();
+                }
+            }
+            // ---- U2: advance every owned pair, four consecutive pairs per thread (a quad never
+            //      straddles two instances: rows are padded to 16); a spike only sets its bit ---------
+            if (ok) {
+                int32_t i = i0, bl = bl0;
+                const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
+                for (int32_t kb = 0; kb < cnt; kb += 4 * U_THREADS) {
+                    const int32_t k = kb + 4 * tid;
+                    const uint32_t kick4 = (kbits[k >> 5] >> sh) & 15u;
+                    uint32_t spk4 = 0;
+                    if (k < cnt && i < n && s_active[bl]) {
+                        AccT x[4];
+                        load4(sacc + k, x);
+                        const float4 v4 = *reinterpret_cast<const float4*>(sv + k);
+                        const float4 g4 = *reinterpret_cast<const float4*>(sg + k);
+                        const uchar4 f4 = *reinterpret_cast<const uchar4*>(sr + k);
+                        float vv[4] = {v4.x, v4.y, v4.z, v4.w}, gg[4] = {g4.x, g4.y, g4.z, g4.w};
+                        uint32_t ff[4] = {f4.x, f4.y, f4.z, f4.w};
+#pragma unroll
+                        for (int j = 0; j < 4; j++) {
+                            if (i + j >= n) continue;
+                            float buf = acc_to_real<float>(x[j], L.w_syn);
+                            const uint32_t f = ff[j];
+                            if (PLASTIC && (f & 0x40)) buf = add_rn(buf, take_plastic<float>(N, S, t, b0 + bl, i + j));
+                            int r = (int)(f & 0x3f);
+                            const bool hb = (f & 0x80) != 0;
+                            const float bias = hb ? S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + S.ext_idx[i + j]] : 0.0f;
+                            if (lif_step<float>(vv[j], gg[j], r, buf, hb, bias, (kick4 >> j) & 1u, L, N.n_ref, N.contract != 0))
+                                spk4 |= 1u << j;
+                            ff[j] = (f & 0xc0) | (uint32_t)r;
+                        }
+                        *reinterpret_cast<float4*>(sv + k) = make_float4(vv[0], vv[1], vv[2], vv[3]);
+                        *reinterpret_cast<float4*>(sg + k) = make_float4(gg[0], gg[1], gg[2], gg[3]);
+                        *reinterpret_cast<uchar4*>(sr + k) =
+                            make_uchar4((uint8_t)ff[0], (uint8_t)ff[1], (uint8_t)ff[2], (uint8_t)ff[3]);
+                    }
+                    // the 8 lanes of a 32-pair word OR their nibbles together; one of them stores it
+                    uint32_t word = spk4 << sh;
+                    word |= __shfl_xor_sync(0xffffffffu, word, 1);
+                    word |= __shfl_xor_sync(0xffffffffu, word, 2);
+                    word |= __shfl_xor_sync(0xffffffffu, word, 4);
+                    if ((lane & 7) == 0) kbits[k >> 5] = word;
+                    i += 4 * U_THREADS;
+                    while (i >= np) { i -= np; bl++; }
+                }
+            }
+            u_sync();
+            // ---- U3: this step's spikes: counts, plastic rows, work items (one atomic per CTA) ----
+            int my_items = 0;
+            for (int32_t w = tid; w < used_words && ok; w += U_THREADS) {
+                uint32_t m = kbits[w];
+                while (m) {
+                    const int32_t k = w * 32 + __ffs(m) - 1;
+                    m &= m - 1;
+                    const int64_t lp = lo + k;
+                    const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
+                    const int32_t b = b0 + bl;
                     A.counts[(int64_t)b * n + i] += 1;
-                    const int64_t len = N.rowptr[i + 1] - N.rowptr[i];
-                    nch = (int)((len + CHUNK - 1) / CHUNK);
+                    my_items += (int)((N.rowptr[i + 1] - N.rowptr[i] + CHUNK - 1) / CHUNK);
                     if (PLASTIC) push_plastic_row(N, S, t, b, i);
                     if (RECORD) {
                         if (A.step_counts) atomicAdd(A.step_counts + (int64_t)s * N.B + b, 1);
@@ -318,21 +362,47 @@ __global__ void __launch_bounds__(PT, 1)
                     }
                 }
             }
-            if (__ballot_sync(0xffffffffu, nch > 0)) warp_append_q(S, slot, q, nch, i, b0 + bl);
-            i += PT;
-            while (i >= np) { i -= (int32_t)np; bl++; }
+            if (my_items) atomicAdd(&s_cnt[0], my_items);
+            u_sync();
+            if (tid == 0 && s_cnt[0] > 0) s_cnt[2] = atomicAdd(count_of(S, slot, q), s_cnt[0]);
+            u_sync();
+            {   // second pass: write the items, and clear every word for the next step's kicks
+                int2* list = list_of(S, slot, q);
+                for (int32_t w = tid; w < used_words; w += U_THREADS) {
+                    uint32_t m = kbits[w];
+                    if (!m) continue;
+                    kbits[w] = 0u;
+                    while (m && ok) {
+                        const int32_t k = w * 32 + __ffs(m) - 1;
+                        m &= m - 1;
+                        const int64_t lp = lo + k;
+                        const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
+                        const int nch = (int)((N.rowptr[i + 1] - N.rowptr[i] + CHUNK - 1) / CHUNK);
+                        if (nch == 0) continue;
+                        const int64_t p0 = (int64_t)s_cnt[2] + atomicAdd(&s_cnt[1], nch);
+                        for (int c = 0; c < nch; c++) {
+                            if (p0 + c < S.cap_g) list[p0 + c] = make_item(N, i, b0 + bl, c);
+                            else atomicExch(err, 1);
+                        }
+                    }
+                }
+            }
+            fence_proxy_async_shared();          // reads of the slice before the next bulk load
+        } else {
+            // ---- P: scatter the spikes that arrive at t+1 into the other accumulator ---------------
+            if (N.n_delay > 1) {
+                AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
+                push_list<AccT, LANES>(N, S, t, q, acc_next, p_tid, p_threads);
+            }
         }
-        fence_proxy_async_shared();          // this step's reads of the slice before the next bulk load
-
-        // (5) scatter the spikes that arrive at t+1 into the other accumulator
-        if (N.n_delay == 1) {
+        if (N.n_delay == 1) {                // P needs this step's spikes: after a grid barrier
             barriers++;
             if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) break;
+            AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
+            push_list<AccT, LANES>(N, S, t, q, acc_next, (int64_t)blockIdx.x * PT + tid, (int64_t)gridDim.x * PT);
         }
-        AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
-        push_list<AccT, LANES>(N, S, t, q, acc_next, gtid, nthreads_grid);
         if (tid == 0 && cnt > 0) {
-            bulk_wait_all();                      // the cleared slice is written before anyone pushes into it
+            bulk_wait_all();                     // the cleared slice is written before anyone pushes into it
             fence_proxy_async_global();
         }
         barriers++;
