@@ -13,6 +13,7 @@
 #include "engine.cuh"
 #include "host_prep.hpp"
 #include "persist.cuh"
+#include "plastic.cuh"
 
 using namespace fb;
 
@@ -132,6 +133,9 @@ struct fb_brain {
     int64_t* pl_rowptr = nullptr;
     int32_t* pl_pidx = nullptr;
     int64_t* pl_q0 = nullptr;
+    int32_t* pl_pre = nullptr;        // presynaptic / postsynaptic neuron of each plastic entry
+    int32_t* pl_post = nullptr;
+    int32_t* ppost_neuron = nullptr;  // neuron of each compact plastic target
     int32_t* ppost_of = nullptr;
     float* pw = nullptr;
     float* w0 = nullptr;
@@ -204,6 +208,7 @@ namespace {
 int free_all(fb_brain* h)
 {
     void* ptrs[] = {h->rowptr, h->col, h->cnt, h->wfx, h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->pw, h->w0,
+                    h->pl_pre, h->pl_post, h->ppost_neuron,
                     h->v, h->g, h->ref, h->ext_idx, h->p_ext, h->bias_ext, h->acc[0], h->acc[1], h->pring,
                     h->items, h->item_count, h->reset_tick, h->stop_tick, h->fly_mask, h->bar, h->abort_flag,
                     h->ext_tab, h->ext_off};
@@ -234,14 +239,19 @@ int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
         CU(cudaMemcpy(old_ring.data(), h->pring, old_ring.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
     }
     std::vector<int64_t> ring = remap_ring(h->plastic, old_ring, P, (int64_t)h->R * B);
-    void* olds[] = {h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->w0, h->pring};
+    void* olds[] = {h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->w0, h->pring, h->pl_pre, h->pl_post,
+                    h->ppost_neuron};
     for (void* p : olds)
         if (p) cudaFree(p);
     if (h->pw) h->graveyard.push_back(h->pw);   // callers may still hold a view of the old weights
     h->pl_rowptr = nullptr; h->pl_pidx = nullptr; h->pl_q0 = nullptr; h->ppost_of = nullptr;
     h->w0 = nullptr; h->pring = nullptr; h->pw = nullptr;
+    h->pl_pre = nullptr; h->pl_post = nullptr; h->ppost_neuron = nullptr;
     size_t* tb = &h->bytes;
     int rc;
+    if ((rc = upload(&h->pl_pre, P.pre, tb))) return rc;
+    if ((rc = upload(&h->pl_post, P.post, tb))) return rc;
+    if ((rc = upload(&h->ppost_neuron, P.ppost_neuron, tb))) return rc;
     if ((rc = upload(&h->pl_rowptr, P.plr, tb))) return rc;
     if ((rc = upload(&h->pl_pidx, P.pl_pidx, tb))) return rc;
     if ((rc = upload(&h->pl_q0, P.q0, tb))) return rc;
@@ -527,6 +537,31 @@ extern "C" int fb_set_plastic(fb_brain* h, const int64_t* pos, int64_t count)
     int rc = install_plastic(h, all);
     if (rc) return rc;
     CU(cudaDeviceSynchronize());
+    return FB_OK;
+}
+
+extern "C" int fb_reward_step(fb_brain* h, const int32_t* counts, double* elig, float* post_mean, const double* coef,
+                              const int32_t* fly_ptr, const int32_t* fly_slots, const float* fly_weight, int32_t n_flies,
+                              const uint8_t* mask, double ae, double ap, float cap, int32_t apply, void* stream)
+{
+    if (!h || !counts || !elig || !post_mean) return fail(FB_ERR_ARG, "NULL argument");
+    if (apply && (!coef || !fly_ptr || !fly_slots || !fly_weight || n_flies <= 0))
+        return fail(FB_ERR_ARG, "apply needs coef, fly_ptr, fly_slots, fly_weight and n_flies > 0");
+    if (h->n_pl == 0) return FB_OK;
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    RewardArgs a{};
+    a.B = h->B; a.n_flies = n_flies; a.n = h->n; a.n_pl = h->n_pl; a.n_ppost = h->n_ppost;
+    a.counts = counts; a.pre = h->pl_pre; a.post = h->pl_post; a.pidx = h->pl_pidx; a.ppost_neuron = h->ppost_neuron;
+    a.w0 = h->w0; a.pw = h->pw; a.elig = elig; a.post_mean = post_mean; a.coef = coef;
+    a.fly_ptr = fly_ptr; a.fly_slots = fly_slots; a.fly_weight = fly_weight; a.mask = mask;
+    a.ae = ae; a.ap = ap; a.cap = cap; a.w_syn = (float)h->params.w_syn; a.apply = apply;
+    k_reward_elig<<<(unsigned)((h->n_pl + 255) / 256), 256, 0, st>>>(a);
+    CU(cudaGetLastError());
+    const int64_t np_ = (int64_t)h->B * h->n_ppost;
+    k_reward_post_mean<<<(unsigned)((np_ + 255) / 256), 256, 0, st>>>(a);
+    CU(cudaGetLastError());
+    h->launches += 2;
     return FB_OK;
 }
 

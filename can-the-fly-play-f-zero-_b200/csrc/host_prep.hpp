@@ -114,6 +114,9 @@ struct PlasticPlan {
     std::vector<int64_t> q0;          // (n_pl) q32 of the connectome weight
     std::vector<float> w0;            // (n_pl) connectome weight f32(count * w_syn)
     std::vector<int32_t> ppost_of;    // (n) compact target index or -1
+    std::vector<int32_t> pre;         // (n_pl) presynaptic neuron of each entry
+    std::vector<int32_t> post;        // (n_pl) postsynaptic neuron of each entry
+    std::vector<int32_t> ppost_neuron;// (n_ppost) neuron of each compact target
 };
 
 // Plan the plastic side for positions `pos` (any order, duplicates allowed). "" or an error.
@@ -143,9 +146,14 @@ inline std::string plan_plastic(const HostCsr& H, std::vector<int64_t> pos, Plas
     up.erase(std::unique(up.begin(), up.end()), up.end());
     for (size_t q = 0; q < up.size(); q++) P.ppost_of[up[q]] = (int32_t)q;
     P.n_ppost = (int32_t)up.size();
+    P.ppost_neuron = up;
+    P.pre.resize(n_pl);
+    P.post.resize(n_pl);
     int64_t r = 0;
     for (int64_t k = 0; k < n_pl; k++) {
         while (H.ip[r + 1] <= pos[k]) r++;          // row containing position pos[k]
+        P.pre[k] = (int32_t)r;
+        P.post[k] = H.ix[pos[k]];
         P.pl_pidx[k] = P.ppost_of[H.ix[pos[k]]];
         P.w0[k] = H.wd[pos[k]];
         P.q0[k] = q32_host(P.w0[k]);

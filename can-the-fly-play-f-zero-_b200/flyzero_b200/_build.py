@@ -17,7 +17,7 @@ CSRC = os.path.join(ROOT, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libflybrain.so")
 SOURCES = ["flybrain.cu", "static_run.cu"]
-HEADERS = ["common.cuh", "engine.cuh", "persist.cuh", "host_prep.hpp"]
+HEADERS = ["common.cuh", "engine.cuh", "persist.cuh", "host_prep.hpp", "plastic.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -60,6 +60,8 @@ SIGNATURES = {
     "fb_run": (C.c_int, [vp, C.c_int32, vp, vp, vp, vp, vp]),
     "fb_set_schedule": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
     "fb_check": (C.c_int, [vp, vp]),
+    "fb_reward_step": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, C.c_int32, vp, C.c_double, C.c_double, C.c_float,
+                                 C.c_int32, vp]),
     "fb_run_static": (C.c_int, [C.POINTER(Params), C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_uint32,
                                 C.c_uint32, C.c_int64, C.c_int32, C.c_int32, vp, vp]),
 }

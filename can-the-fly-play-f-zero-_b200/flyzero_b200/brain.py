@@ -155,7 +155,19 @@ class Brain:
             if len(self.input_idx):
                 e.p_ext[0, torch.as_tensor(e._slot[self.input_idx], device=e.device)] = torch.as_tensor(
                     p_in, device=e.device)
-        counts = e.run_steps(steps, kicks)[0].cpu().numpy()
+        dev_counts = e.run_steps(steps, kicks)
+        counts = dev_counts[0].cpu().numpy()
+        self._last = (counts, dev_counts)
         self.t += steps
         self.spike_count += counts
         return counts
+
+    def device_counts(self, counts: np.ndarray):
+        """(1, n) int32 device tensor of ``counts``: the engine's own copy if ``counts`` is what the
+        last ``run`` returned, else an upload."""
+        import torch
+
+        last = getattr(self, "_last", None)
+        if last is not None and last[0] is counts:
+            return last[1]
+        return torch.as_tensor(np.asarray(counts, np.int32).reshape(1, -1), device=self._eng.device)

@@ -136,6 +136,25 @@ int fb_reset(fb_brain* brain, const int32_t* flies /*[host]*/, int32_t n_flies, 
 int fb_run(fb_brain* brain, int32_t steps, int32_t* counts_out, const uint32_t* kicks,
            int32_t* step_counts, uint64_t* step_digest, void* stream);
 
+/* The reward-modulated plastic update of every instance, fused on the device (two launches).
+ * Restates RewardPlasticity.step (flyzero/learning.py:116-131) for one instance and
+ * BatchReward.step + _Plastic.apply (flyzero/batch.py:158-172, 482-495) for many:
+ *   E = ae*E + c[pre]*(c[post] - <post>);  per fly f: s_f = sum_{learning b of f} fly_weight[b]*coef[b]*E_b;
+ *   every slot b of fly f: pw = sign*clip(sign*(pw + s_f), 0, cap*max(|w0|, w_syn));
+ *   <post> += ap*(c[post] - <post>).
+ *   counts     [device] (batch, n) int32 spike counts of the window just run
+ *   elig       [device] (batch, n_plastic) float64 eligibility traces, updated in place
+ *   post_mean  [device] (batch, n_targets) float32 running mean count of each plastic target
+ *              (targets = distinct postsynaptic neurons of the plastic entries, ascending)
+ *   coef       [device] (batch) float64: eta * advantage of each slot, rounded as the rule does
+ *   fly_ptr    [device] (n_flies+1), fly_slots [device] (batch): slots grouped by fly
+ *   fly_weight [device] (batch) float32: 1/(learning slots of the fly) for a learning slot, else 0
+ *   mask       [device] NULL or (n_plastic) uint8: the plastic entries this rule owns (others untouched)
+ *   apply      0: traces and means only (no slot learns this frame, batch.py:493) */
+int fb_reward_step(fb_brain* brain, const int32_t* counts, double* elig, float* post_mean, const double* coef,
+                   const int32_t* fly_ptr, const int32_t* fly_slots, const float* fly_weight, int32_t n_flies,
+                   const uint8_t* mask, double ae, double ap, float cap, int32_t apply, void* stream);
+
 /* Choose the schedule (FB_ENGINE_*, FB_PROP_*, lanes per work item 8/16/32; 0 keeps a field). */
 int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
 

@@ -104,7 +104,9 @@ int main()
                 int64_t row = 0;
                 while (c.ip[row + 1] <= p) row++;
                 CHECK(P->plr[row] <= k && k < P->plr[row + 1]);
+                CHECK(P->pre[k] == row && P->post[k] == H.ix[p]);
                 CHECK(P->ppost_of[H.ix[p]] == P->pl_pidx[k]);
+                CHECK(P->ppost_neuron[P->pl_pidx[k]] == H.ix[p]);
                 CHECK(P->w0[k] == H.wd[p] && P->q0[k] == q32_host(H.wd[p]));
             }
         }
