@@ -11,8 +11,9 @@
 //   inputs      ext_idx[n] i32, p_ext[B][n_ext] f32, bias_ext[B][n_ext] f32
 //   delay line  acc[2][B][n_pad] (i32 or i64): synaptic input of the next two steps, rows padded
 //               to 16 entries so that every row starts on a 64-byte boundary (TMA bulk copies);
-//               items[R][n_groups][cap_g] int2: spike work lists of the last R = n_delay+1 steps,
-//               one list per instance group; pring[R][B][n_ppost] i64: plastic input
+//               items[R][n_groups][n_seg][cap_c] int2: spike work lists of the last R = n_delay+1
+//               steps, one per instance group and segment (the pairs one persistent CTA owns);
+//               item_count[R][n_groups][n_seg]; pring[R][B][n_ppost] i64: plastic input
 //
 // The delay line is "deferred push": the fixed-weight rows of the spikes of step s are scattered
 // into acc only at step s + n_delay - 1, right before they arrive, so only two accumulator slots
@@ -27,7 +28,6 @@ namespace fb {
 struct DevNet {
     int64_t n, n_pad;
     int32_t B, n_delay, R, n_ref;
-    int32_t contract;
     const int64_t* rowptr;
     const int32_t* col;
     const int16_t* cnt;
@@ -54,11 +54,13 @@ struct DevState {
     void* acc0;
     void* acc1;
     int64_t* pring;
-    int2* items;
-    int32_t* item_count;       // [R][n_groups]
-    int64_t cap_g;             // items per (step, group) list
-    int32_t group;             // instances per group (list owner = b / group)
+    int2* items;               // [R][n_groups][n_seg][cap_c]
+    int32_t* item_count;       // [R][n_groups][n_seg]
+    int64_t cap_c;             // items per (step, group, segment) list
+    int32_t group;             // instances per group (group of instance b = b / group)
     int32_t n_groups;
+    int32_t n_seg;             // segments per group: the CTAs of the persistent plan (1 without one)
+    int64_t seg_pairs;         // pairs per segment; pair (b, i) = (b mod group) * n_pad + i
     const int64_t* reset_tick;
     const int64_t* stop_tick;
     int32_t* err;              // [0] overflow, [1] barrier timeout step (host-mapped)
@@ -88,13 +90,33 @@ template <typename Real> __device__ __forceinline__ const Lif<Real>& lif_of(cons
 template <> __device__ __forceinline__ const Lif<float>& lif_of<float>(const DevNet& N) { return N.L32; }
 template <> __device__ __forceinline__ const Lif<double>& lif_of<double>(const DevNet& N) { return N.L64; }
 
-__device__ __forceinline__ int2* list_of(const DevState& S, int64_t slot, int32_t q)
+__device__ __forceinline__ int2* list_of(const DevState& S, int64_t slot, int32_t q, int32_t c)
 {
-    return S.items + ((int64_t)slot * S.n_groups + q) * S.cap_g;
+    return S.items + (((int64_t)slot * S.n_groups + q) * S.n_seg + c) * S.cap_c;
 }
-__device__ __forceinline__ int32_t* count_of(const DevState& S, int64_t slot, int32_t q)
+__device__ __forceinline__ int32_t* count_of(const DevState& S, int64_t slot, int32_t q, int32_t c)
 {
-    return S.item_count + (int64_t)slot * S.n_groups + q;
+    return S.item_count + ((int64_t)slot * S.n_groups + q) * S.n_seg + c;
+}
+// list key (group * n_seg + segment) of the pair (b, i)
+__device__ __forceinline__ int32_t list_key(const DevState& S, int64_t n_pad, int32_t b, int32_t i)
+{
+    const int32_t q = b / S.group;
+    const int64_t p = (int64_t)(b - q * S.group) * n_pad + i;
+    return q * S.n_seg + (int32_t)(p / S.seg_pairs);
+}
+
+// Fire-and-forget reductions into global memory (no value comes back; the address is converted to
+// the global window explicitly, so the hardware never falls back to a returning generic atomic).
+// No "memory" clobber: the reduced words are never read in the phase that reduces into them, and
+// leaving the clobber out lets the compiler issue the next edges' loads before these reductions.
+__device__ __forceinline__ void red_add(int32_t* p, int32_t x)
+{
+    asm volatile("red.relaxed.gpu.global.add.s32 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(x));
+}
+__device__ __forceinline__ void red_add(int64_t* p, int64_t x)
+{
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "l"(x));
 }
 
 // A work item: up to CHUNK consecutive entries of a spiking row, {first entry in the padded CSR,
@@ -106,19 +128,20 @@ __device__ __forceinline__ int2 make_item(const DevNet& N, int32_t i, int32_t b,
     return make_int2((int32_t)k0, (b << CHUNK_BITS) | (int32_t)min((int64_t)CHUNK, r1 - k0));
 }
 
-// Append `nch` work items (this lane's spike: chunks 0..nch-1 of row i of instance b) to the list
-// of the lane's instance group; one atomic per warp and group (the ballot/shuffle compaction).
+// Append `nch` work items (this lane's spike: chunks 0..nch-1 of row i of instance b) to the list of
+// the lane's (group, segment); one atomic per warp and list (the ballot/shuffle compaction).
 __device__ __forceinline__ void warp_append(const DevNet& N, const DevState& S, int64_t slot, int nch, int32_t i,
                                             int32_t b)
 {
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     unsigned todo = __ballot_sync(FULL, nch > 0);
-    const int32_t q = b / S.group;
+    if (!todo) return;
+    const int32_t key = nch > 0 ? list_key(S, N.n_pad, b, i) : -1;
     while (todo) {
         const int leader = __ffs(todo) - 1;
-        const int32_t qq = __shfl_sync(FULL, q, leader);
-        const bool mine = nch > 0 && q == qq;
+        const int32_t kk = __shfl_sync(FULL, key, leader);
+        const bool mine = nch > 0 && key == kk;
         int incl = mine ? nch : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -126,15 +149,16 @@ __device__ __forceinline__ void warp_append(const DevNet& N, const DevState& S, 
             if (lane >= o) incl += y;
         }
         const int total = __shfl_sync(FULL, incl, 31);
+        const int32_t q = kk / S.n_seg, c = kk - q * S.n_seg;
         int base = 0;
-        if (lane == 31) base = atomicAdd(count_of(S, slot, qq), total);
+        if (lane == 31) base = atomicAdd(count_of(S, slot, q, c), total);
         base = __shfl_sync(FULL, base, 31);
         if (mine) {
-            int2* list = list_of(S, slot, qq);
+            int2* list = list_of(S, slot, q, c);
             const int64_t start = (int64_t)base + incl - nch;
-            for (int c = 0; c < nch; c++) {
-                const int64_t p = start + c;
-                if (p < S.cap_g) list[p] = make_item(N, i, b, c);
+            for (int ch = 0; ch < nch; ch++) {
+                const int64_t p = start + ch;
+                if (p < S.cap_c) list[p] = make_item(N, i, b, ch);
                 else atomicExch(S.err, 1);
             }
         }
@@ -152,7 +176,7 @@ __device__ __forceinline__ void push_plastic_row(const DevNet& N, const DevState
     const float* w = S.pw + (int64_t)b * N.n_pl;
     for (int64_t k = p0; k < p1; k++) {
         const int64_t d = to_q32(w[k]) - N.pl_q0[k];
-        if (d != 0) atomicAdd(dst + N.pl_pidx[k], (unsigned long long)d);
+        if (d != 0) red_add(reinterpret_cast<int64_t*>(dst) + N.pl_pidx[k], d);
     }
 }
 
@@ -190,8 +214,9 @@ __global__ void __launch_bounds__(256) k_update(const DevNet N, const DevState S
     const int64_t total = (int64_t)N.B * n;
     const Lif<Real>& L = lif_of<Real>(N);
     const int64_t t = A.t;
-    if (blockIdx.x == 0 && threadIdx.x < S.n_groups)
-        *count_of(S, pos_mod(t - N.n_delay, N.R), threadIdx.x) = 0;   // consumed by the push at t-1
+    if (blockIdx.x == 0)       // the lists consumed by the push at t-1 start empty again
+        for (int32_t k = threadIdx.x; k < S.n_groups * S.n_seg; k += blockDim.x)
+            S.item_count[pos_mod(t - N.n_delay, N.R) * S.n_groups * S.n_seg + k] = 0;
     AccT* acc = reinterpret_cast<AccT*>((t & 1) ? S.acc1 : S.acc0);
     Real* V = reinterpret_cast<Real*>(S.v);
     Real* G = reinterpret_cast<Real*>(S.g);
@@ -221,7 +246,8 @@ __global__ void __launch_bounds__(256) k_update(const DevNet N, const DevState S
                     bias = S.bias_ext[(int64_t)b * S.n_ext + j];
                     kicked = kick_of<RASTER>(S, A.kicks, A.words, N.B, A.s, b, j, (uint32_t)pair, A.step_no);
                 }
-                const bool spk = lif_step<Real>(v, g, r, buf, j >= 0, bias, kicked, L, N.n_ref, N.contract != 0);
+                // the engine always fuses the two multiply-adds, as the shipped reference kernel does
+                const bool spk = lif_step<Real>(v, g, r, buf, j >= 0, bias, kicked, L, N.n_ref, true);
                 if (bits_differ(g, g0)) G[pair] = g;
                 if (bits_differ(v, v0)) V[pair] = v;
                 if (r != r0) S.ref[pair] = (int8_t)r;
@@ -282,17 +308,12 @@ template <> struct Edges8<int64_t> {
     }
 };
 
-__device__ __forceinline__ void red_add(int32_t* p, int32_t x) { atomicAdd(p, x); }
-__device__ __forceinline__ void red_add(int64_t* p, int64_t x)
-{
-    atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)x);
-}
-
 // Scatter one work item (<= CHUNK entries of a spiking row) with LANES lanes, 8 entries a lane.
 template <typename AccT, int LANES>
 __device__ __forceinline__ void push_item(const DevNet& N, AccT* acc_b, int64_t k0, int32_t len, int lane)
 {
     const int64_t k1 = k0 + len;
+#pragma unroll 2
     for (int64_t k = k0 + (int64_t)lane * 8; k < k1; k += LANES * 8) {
         Edges8<AccT> e;
         e.load(N, k);
@@ -302,23 +323,70 @@ __device__ __forceinline__ void push_item(const DevNet& N, AccT* acc_b, int64_t 
     }
 }
 
-// Scatter the group-q list of spike step s (arriving at tick t+1) into acc_next, `ngroups_total`
-// groups of LANES lanes striding over the items. Lists are read through L2 (other SMs wrote them).
+// Inclusive prefix over the n_seg segment counts of list (slot, q) into `pre` (shared memory),
+// computed by one warp (n_seg <= MAX_SEG); returns the total. Counts are clamped to the capacity.
+constexpr int MAX_SEG = 256;
+__device__ __forceinline__ int32_t segment_prefix(const DevState& S, int64_t slot, int32_t q, int32_t* pre)
+{
+    constexpr int PER_LANE = MAX_SEG / 32;
+    const int lane = threadIdx.x & 31;
+    const int32_t* cnt = count_of(S, slot, q, 0);
+    const int32_t c0 = lane * PER_LANE;
+    int32_t x[PER_LANE];
+#pragma unroll
+    for (int j = 0; j < PER_LANE; j++) x[j] = c0 + j < S.n_seg ? __ldcg(cnt + c0 + j) : 0;   // all in flight
+    int32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER_LANE; j++) {
+        x[j] = (int32_t)min((int64_t)max(x[j], 0), S.cap_c);
+        sum += x[j];
+    }
+    int32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    int32_t run = incl - sum;
+#pragma unroll
+    for (int j = 0; j < PER_LANE; j++) {
+        run += x[j];
+        if (c0 + j < S.n_seg) pre[c0 + j] = run;
+    }
+    return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+// Scatter the items [g0, g1) of list (slot of spike step s = t+1-n_delay, group q) into acc_next.
+// The list is the concatenation of its segments, described by their inclusive prefix `pre`; lane
+// group `lg` of `n_lg` (LANES lanes each, lane `lane` within it) takes items g0+lg, g0+lg+n_lg, ...
+// and follows the segment boundaries forward (a search only when it crosses one). Items of
+// instance b are skipped unless reset_tick[b - b_base] <= s and t+1 < stop_tick[b - b_base].
 template <typename AccT, int LANES>
-__device__ __forceinline__ void push_list(const DevNet& N, const DevState& S, int64_t t, int32_t q, AccT* acc_next,
-                                          int64_t gtid, int64_t nthreads)
+__device__ __forceinline__ void push_range(const DevNet& N, const DevState& S, int64_t t, int32_t q, AccT* acc_next,
+                                           const int32_t* pre, int64_t g0, int64_t g1, int64_t lg, int64_t n_lg,
+                                           int lane, const int64_t* reset_tick, const int64_t* stop_tick,
+                                           int32_t b_base)
 {
     const int64_t s = t + 1 - N.n_delay;
     if (s < 0) return;
     const int64_t slot = pos_mod(s, N.R);
-    const int64_t n_items = min((int64_t)__ldcg(count_of(S, slot, q)), S.cap_g);
-    const int2* list = list_of(S, slot, q);
-    const int lane = (int)(gtid % LANES);
-    const int64_t ngroups = nthreads / LANES;
-    for (int64_t it = gtid / LANES; it < n_items; it += ngroups) {
-        const int2 item = __ldcg(list + it);
+    int32_t seg = -1;
+    int64_t seg_lo = 0, seg_hi = 0;
+    for (int64_t g = g0 + lg; g < g1; g += n_lg) {
+        if (g >= seg_hi) {                        // first segment whose prefix exceeds g
+            int32_t lo = seg + 1, hi = S.n_seg - 1;
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (pre[mid] > g) hi = mid;
+                else lo = mid + 1;
+            }
+            seg = lo;
+            seg_lo = lo > 0 ? pre[lo - 1] : 0;
+            seg_hi = pre[lo];
+        }
+        const int2 item = __ldcg(list_of(S, slot, q, seg) + (g - seg_lo));
         const int32_t b = item.y >> CHUNK_BITS;
-        if (s < S.reset_tick[b] || t + 1 >= S.stop_tick[b]) continue;
+        if (s < reset_tick[b - b_base] || t + 1 >= stop_tick[b - b_base]) continue;
         push_item<AccT, LANES>(N, acc_next + (int64_t)b * N.n_pad, (int64_t)(uint32_t)item.x,
                                item.y & ((1 << CHUNK_BITS) - 1), lane);
     }
@@ -326,15 +394,28 @@ __device__ __forceinline__ void push_list(const DevNet& N, const DevState& S, in
 
 // ---------------------------------------------------------------------------------------------
 // Step engine, kernel 2: the spikes of step t+1-n_delay (they arrive at step t+1) are scattered
-// into the accumulator that step t+1 reads. LANES lanes per work item.
+// into the accumulator that step t+1 reads; each block takes a contiguous share of every list.
 // ---------------------------------------------------------------------------------------------
 template <typename AccT, int LANES>
 __global__ void __launch_bounds__(256) k_push(const DevNet N, const DevState S, int64_t t)
 {
+    __shared__ int32_t pre[MAX_SEG];
+    __shared__ int32_t s_total;
+    if (t + 1 - N.n_delay < 0) return;
     AccT* acc = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
-    const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
-    for (int32_t q = 0; q < S.n_groups; q++) push_list<AccT, LANES>(N, S, t, q, acc, gtid, nthreads);
+    const int64_t slot = pos_mod(t + 1 - N.n_delay, N.R);
+    for (int32_t q = 0; q < S.n_groups; q++) {
+        if (threadIdx.x < 32) {
+            const int32_t tot = segment_prefix(S, slot, q, pre);
+            if (threadIdx.x == 0) s_total = tot;
+        }
+        __syncthreads();
+        const int64_t total = s_total;
+        const int64_t g0 = total * blockIdx.x / gridDim.x, g1 = total * (blockIdx.x + 1) / gridDim.x;
+        push_range<AccT, LANES>(N, S, t, q, acc, pre, g0, g1, threadIdx.x / LANES, blockDim.x / LANES,
+                                threadIdx.x % LANES, S.reset_tick, S.stop_tick, 0);
+        __syncthreads();
+    }
 }
 
 }  // namespace fb

@@ -116,7 +116,6 @@ struct fb_brain {
     int32_t B = 0, n_delay = 1, n_ref = 0, R = 2;
     int acc_mode = 0;      // 0 INT32 counts, 1 Q32.32
     int f64 = 0;
-    int contract = 1;
     uint32_t seed = 0;
     double consts64[3] = {0, 0, 0};
     Lif<float> L32{};
@@ -157,9 +156,11 @@ struct fb_brain {
     int64_t* pring = nullptr;
     int2* items = nullptr;
     int32_t* item_count = nullptr;
-    int64_t cap_g = 0;            // items per (step, group) list
-    int32_t list_group = 1;       // instances per list (the persistent group size, or B)
+    int64_t cap_c = 0;            // items per (step, group, segment) list
+    int32_t list_group = 1;       // instances per group (the persistent group size, or B)
     int32_t n_groups = 1;
+    int32_t n_seg = 1;            // segments per group (the persistent CTAs, or 1)
+    int64_t seg_pairs = 0;        // pairs per segment
     unsigned int* bar = nullptr;  // persistent grid-barrier counter
     int32_t* abort_flag = nullptr;
     int2* ext_tab = nullptr;      // persistent engine: input pairs of each CTA
@@ -167,6 +168,8 @@ struct fb_brain {
     int64_t* reset_tick = nullptr;
     int64_t* stop_tick = nullptr;
     uint8_t* fly_mask = nullptr;
+    long long* trace = nullptr;   // caller's phase-trace buffer (fb_set_trace) or nullptr
+    int64_t trace_cap = 0;
     int32_t* err_h = nullptr;   // host-mapped flags
     int32_t* err_d = nullptr;
     // counters
@@ -184,7 +187,7 @@ struct fb_brain {
     DevNet net() const
     {
         DevNet N{};
-        N.n = n; N.n_pad = n_pad; N.B = B; N.n_delay = n_delay; N.R = R; N.n_ref = n_ref; N.contract = contract;
+        N.n = n; N.n_pad = n_pad; N.B = B; N.n_delay = n_delay; N.R = R; N.n_ref = n_ref;
         N.rowptr = rowptr; N.col = col; N.cnt = cnt; N.wfx = wfx;
         N.n_pl = n_pl; N.n_ppost = n_ppost; N.pl_rowptr = pl_rowptr; N.pl_pidx = pl_pidx; N.pl_q0 = pl_q0;
         N.ppost_of = ppost_of;
@@ -196,8 +199,8 @@ struct fb_brain {
         DevState S{};
         S.v = v; S.g = g; S.ref = ref; S.pw = pw; S.ext_idx = ext_idx; S.n_ext = (int32_t)n_ext;
         S.p_ext = p_ext; S.bias_ext = bias_ext; S.acc0 = acc[0]; S.acc1 = acc[1]; S.pring = pring;
-        S.items = items; S.item_count = item_count; S.cap_g = cap_g; S.group = list_group;
-        S.n_groups = n_groups; S.reset_tick = reset_tick;
+        S.items = items; S.item_count = item_count; S.cap_c = cap_c; S.group = list_group;
+        S.n_groups = n_groups; S.n_seg = n_seg; S.seg_pairs = seg_pairs; S.reset_tick = reset_tick;
         S.stop_tick = stop_tick; S.err = err_d; S.seed = seed;
         return S;
     }
@@ -372,15 +375,18 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
     TRY(dalloc(&h->bar, 1, tb));
     TRY(dalloc(&h->abort_flag, 1, tb));
     int dev_sms2 = h->sm_count;
-    h->plan = plan_persistent(h->n, h->n_pad, h->B, h->f64 != 0, h->n_ref, (int)ab, dev_sms2, h->device);
+    h->plan = plan_persistent(h->n, h->n_pad, h->B, h->f64 != 0, h->n_ref, h->n_delay, (int)ab, dev_sms2, h->device);
     h->list_group = h->plan.group > 0 ? h->plan.group : h->B;
     h->n_groups = (h->B + h->list_group - 1) / h->list_group;
     TRY(install_plastic(h, pos));
     TRY(build_ext_table(h));
-    // worst case: every neuron of every instance of a group fires in the same step
-    h->cap_g = std::max<int64_t>(1, H.chunks_all * h->list_group);
-    TRY(dalloc(&h->items, (size_t)h->R * h->n_groups * h->cap_g, tb));
-    TRY(dalloc(&h->item_count, (size_t)h->R * h->n_groups, tb));
+    // one list segment per persistent CTA (the pairs it owns); capacity for the worst case, every
+    // pair of the segment firing in the same step
+    h->n_seg = h->plan.group > 0 ? h->plan.ctas : 1;
+    h->seg_pairs = h->plan.group > 0 ? h->plan.per : (int64_t)h->list_group * h->n_pad;
+    h->cap_c = segment_capacity(H, h->n_pad, h->list_group, h->seg_pairs, h->n_seg);
+    TRY(dalloc(&h->items, (size_t)h->R * h->n_groups * h->n_seg * h->cap_c, tb));
+    TRY(dalloc(&h->item_count, (size_t)h->R * h->n_groups * h->n_seg, tb));
     TRY(dalloc(&h->reset_tick, (size_t)batch, tb));
     TRY(dalloc(&h->stop_tick, (size_t)batch, tb));
     TRY(dalloc(&h->fly_mask, (size_t)batch, tb));
@@ -431,7 +437,7 @@ extern "C" int fb_get_info(const fb_brain* h, fb_info* o)
     o->acc_mode = h->acc_mode; o->f64 = h->f64; o->engine = h->engine; o->propagation = h->prop;
     o->lanes = h->lanes; o->group = h->plan.group; o->ctas = h->plan.ctas; o->n_plastic = h->n_pl;
     o->n_ext = h->n_ext; o->t = h->t; o->step_no = h->step_no; o->launches = h->launches;
-    o->item_capacity = h->cap_g; o->bytes_device = (int64_t)h->bytes;
+    o->item_capacity = h->cap_c; o->bytes_device = (int64_t)h->bytes;
     o->decay_syn = h->consts64[0]; o->decay_m = h->consts64[1]; o->kick = h->consts64[2];
     return FB_OK;
 }
@@ -513,7 +519,7 @@ extern "C" int fb_reset(fb_brain* h, const int32_t* flies, int32_t n_flies, void
     h->launches += 1;
     if (all) {
         h->t = 0;
-        CU(cudaMemsetAsync(h->item_count, 0, (size_t)h->R * h->n_groups * sizeof(int32_t), st));
+        CU(cudaMemsetAsync(h->item_count, 0, (size_t)h->R * h->n_groups * h->n_seg * sizeof(int32_t), st));
     }
     k_set_ticks<<<(h->B + 255) / 256, 256, 0, st>>>(h->reset_tick, mask, h->B, h->t);
     CU(cudaGetLastError());
@@ -581,6 +587,15 @@ extern "C" int fb_set_schedule(fb_brain* h, int32_t engine, int32_t propagation,
     return FB_OK;
 }
 
+extern "C" int fb_set_trace(fb_brain* h, long long* trace, int64_t capacity)
+{
+    if (!h) return fail(FB_ERR_ARG, "NULL brain");
+    if (trace && capacity <= 0) return fail(FB_ERR_ARG, "capacity must be > 0");
+    h->trace = trace;
+    h->trace_cap = trace ? capacity : 0;
+    return FB_OK;
+}
+
 extern "C" int fb_check(fb_brain* h, void* stream)
 {
     if (!h) return fail(FB_ERR_ARG, "NULL brain");
@@ -588,7 +603,7 @@ extern "C" int fb_check(fb_brain* h, void* stream)
     CU(cudaStreamSynchronize((cudaStream_t)stream));
     const int32_t over = h->err_h[0], tmo = h->err_h[1];
     h->err_h[0] = h->err_h[1] = 0;
-    if (over) return fail(FB_ERR_OVERFLOW, "spike work list overflowed its capacity of %lld items", (long long)h->cap_g);
+    if (over) return fail(FB_ERR_OVERFLOW, "spike work list overflowed its capacity of %lld items", (long long)h->cap_c);
     if (tmo) return fail(FB_ERR_TIMEOUT, "a grid-barrier wait ran out of its budget (step %d)", tmo);
     return FB_OK;
 }
@@ -670,6 +685,7 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         P.t0 = h->t; P.step0 = h->step_no; P.steps = steps; P.kicks = kicks; P.words = words;
         P.counts = counts_out; P.step_counts = step_counts; P.step_digest = step_digest;
         P.bar = h->bar; P.abort_flag = h->abort_flag; P.ext_tab = h->ext_tab; P.ext_off = h->ext_off;
+        P.trace = ((int64_t)steps * h->plan.ctas * TRACE_SLOTS <= h->trace_cap) ? h->trace : nullptr;
         CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
         int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
                                    record, h->lanes, st);

@@ -30,7 +30,26 @@ struct HostCsr {
     std::vector<int64_t> pwfx;        // (nnz_pad) Q32.32 weights (acc_mode 1), padding 0
     int32_t max_chunks = 0;           // work items of the longest padded row
     int64_t chunks_all = 0;           // work items if every neuron fires (sum over padded rows)
+    std::vector<int64_t> chunk_cum;   // (n+1) work items of rows 0..i-1
 };
+
+// Work items if every pair of one list segment fires, maximised over the segments: segment c holds
+// the pairs [c * seg_pairs, (c+1) * seg_pairs) of a group of `group` instances (pair (b, i) =
+// b * n_pad + i; pairs with i >= n are padding and never fire).
+inline int64_t segment_capacity(const HostCsr& H, int64_t n_pad, int64_t group, int64_t seg_pairs, int64_t n_seg)
+{
+    auto upto = [&](int64_t p) {                  // items of the pairs [0, p)
+        const int64_t b = p / n_pad, i = std::min(p - b * n_pad, H.n);
+        return b * H.chunks_all + H.chunk_cum[i];
+    };
+    const int64_t pairs = group * n_pad;
+    int64_t cap = 1;
+    for (int64_t c = 0; c < n_seg; c++) {
+        const int64_t lo = std::min(c * seg_pairs, pairs), hi = std::min(lo + seg_pairs, pairs);
+        cap = std::max(cap, upto(hi) - upto(lo));
+    }
+    return cap;
+}
 
 // Returns "" on success or the error message.
 inline std::string prepare_csr(const int64_t* indptr, const int32_t* indices, const float* data, int64_t n,
@@ -77,6 +96,7 @@ inline std::string prepare_csr(const int64_t* indptr, const int32_t* indices, co
     for (int64_t k = 0; k < nnz; k++) H.wd[k] = dv[k] * w_syn32;
 
     H.rp.assign(n + 1, 0);
+    H.chunk_cum.assign(n + 1, 0);
     int64_t max_pad = 0;
     for (int64_t i = 0; i < n; i++) {
         const int64_t len = H.ip[i + 1] - H.ip[i];
@@ -84,6 +104,7 @@ inline std::string prepare_csr(const int64_t* indptr, const int32_t* indices, co
         H.rp[i + 1] = H.rp[i] + padded;
         max_pad = std::max(max_pad, padded);
         H.chunks_all += (padded + HOST_CHUNK - 1) / HOST_CHUNK;
+        H.chunk_cum[i + 1] = H.chunks_all;
     }
     H.nnz_pad = H.rp[n];
     H.max_chunks = (int32_t)((max_pad + HOST_CHUNK - 1) / HOST_CHUNK);

@@ -2,16 +2,23 @@
 //
 // Instances are independent, so B is split into groups small enough that a group's neuron state
 // (v, g f32 + refractory/flag byte = 9 B per instance-neuron) fits in the shared memory of the
-// whole GPU (~148 x 200 KB). Each CTA owns a contiguous slice of the group's (instance, neuron)
-// pairs and keeps its state in shared memory for the whole run: per step, HBM/L2 traffic is only
-// the synaptic-input accumulator (read + clear, staged into shared memory by TMA 1-D bulk
-// copies, 3 stages of 16 KB), the CSR rows of spiking neurons and the atomics they scatter.
+// whole GPU (148 x ~200 KB). Each CTA owns a contiguous slice of the group's (instance, neuron)
+// pairs and keeps their state in shared memory for the whole run: per step, HBM/L2 traffic is
+// only the synaptic-input accumulator slice (one TMA bulk load into shared memory, cleared behind
+// it by bulk stores from a zero page), the CSR rows of the spikes that arrive next step, and the
+// reductions they scatter.
 //
-// Per step, every CTA: (U) advances its pairs, compacts spikes into the group's work list;
-// (P) scatters the list of the spikes that arrive next step into the other accumulator;
-// then a grid barrier (bounded: after ~4 s it raises the timeout flag and every CTA returns).
-// U of step t and P of step t touch different accumulators, so one barrier per step suffices
-// (two when n_delay == 1, where P needs this step's spikes).
+// Warp roles of a CTA (all steps, separated by one grid barrier per step):
+//   neuron warps (U, 28): stage the slice, advance every owned pair, then draw the next step's
+//     Poisson kicks into a shared bitmap;
+//   push warps (2): scatter the work items that arrive next step into the other accumulator;
+//   listing warps (2): list the previous step's spikes (counts, plastic rows, work items of this
+//     CTA's segment of the group's list).
+// A spike of step s is listed during step s+1 and first scattered during step s+n_delay-1, so
+// the engine needs n_delay >= 3. Three bitmaps rotate: map[s%3] holds the kicks of step s, then
+// (overwritten by the neuron warps) its spikes; map[(s+1)%3] receives the next kicks; the listing
+// warps read and clear map[(s-1)%3]. Every wait is bounded: after ~4 s a CTA raises the timeout
+// flag and every CTA returns.
 #pragma once
 #include "engine.cuh"
 
@@ -20,7 +27,14 @@ namespace fb {
 constexpr int PT = 1024;                // threads per CTA
 constexpr int ZERO_PAGE = 4096;         // shared-memory zeros, the source of the clearing bulk stores
 constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulator slice
+constexpr int SPK_BUF = 1024;           // spikes of one CTA and step listed in parallel
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
+
+constexpr int PUSH_WARPS = 2;                              // warps that scatter arriving items ...
+constexpr int LIST_WARPS = 2;                              // ... that list the previous step's spikes ...
+constexpr int PUSH_THREADS = 32 * PUSH_WARPS;
+constexpr int LIST_THREADS = 32 * LIST_WARPS;
+constexpr int U_THREADS = PT - PUSH_THREADS - LIST_THREADS;   // ... and the rest advance neurons
 
 struct PersistPlan {
     int32_t group = 0;        // instances per launch (0: engine unavailable)
@@ -44,7 +58,14 @@ struct PersistArgs {
     int32_t* abort_flag;      // zeroed before the launch
     const int2* ext_tab;      // per CTA: input pairs {k | instance << 18, ext slot}
     const int32_t* ext_off;   // (ctas + 1) offsets into ext_tab
+    long long* trace;         // nullptr, or (steps, ctas, TRACE_SLOTS) clock64 stamps of each step's phases
 };
+
+// Phase stamps (per step and CTA; SM clock cycles, compare within a CTA): 0 step start, 1 neuron
+// warps start, 2 slice in shared memory, 3 neurons advanced, 4 next kicks drawn, 5 barrier
+// arrival of the neuron warps, 6 barrier exit, 7 push warps start, 8 listing warps done,
+// 9 push warps' segment prefix ready, 10 push warps done.
+constexpr int TRACE_SLOTS = 11;
 
 // ---- PTX helpers: mbarrier, TMA 1-D bulk copy, proxy fences, acquire load --------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -87,6 +108,12 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p)
     return v;
 }
 __device__ __forceinline__ int ld_volatile_i32(const int32_t* p) { return *reinterpret_cast<const volatile int32_t*>(p); }
+
+
+__device__ __forceinline__ void stamp(const PersistArgs& A, int32_t s, int slot)
+{
+    if (A.trace) A.trace[((int64_t)s * gridDim.x + blockIdx.x) * TRACE_SLOTS + slot] = clock64();
+}
 
 // Grid barrier with a bounded wait. Returns true if the run must stop (timeout here or elsewhere).
 __device__ __forceinline__ bool grid_barrier(const PersistArgs& A, unsigned int target, int32_t* err, int tag)
@@ -131,24 +158,25 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
 
 // Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
 struct PersistSmem {
-    int64_t mbar, zero, acc, v, g, kbits, ref, misc, total;
+    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, total, words_per_map;
     __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
     {
-        const int64_t words = (per + 4 * PT) / 32 + 1;
+        words_per_map = (per + 4 * PT) / 32 + 1;
         mbar = 0;
         zero = 128;
         acc = zero + ZERO_PAGE;
         v = acc + per * acc_bytes;
         g = v + per * 4;
-        kbits = g + per * 4;
-        ref = kbits + words * 4;
-        misc = (ref + per + 15) / 16 * 16;   // 64 active flags + 4 counters
-        total = misc + 64 + 16;
+        kbits = g + per * 4;                 // three bitmaps: the kicks of a step become its spikes
+        ref = kbits + 3 * words_per_map * 4;
+        misc = (ref + per + 15) / 16 * 16;   // 64 active flags, 8 counters
+        scan = misc + 64 + 32;               // 32 block-scan partial sums
+        pre = scan + 128;                    // 2 x MAX_SEG segment prefix entries (step parity)
+        spk = pre + 8 * MAX_SEG;             // SPK_BUF spikes being listed
+        ticks = spk + 4 * SPK_BUF;           // reset and stop ticks of up to 64 instances
+        total = ticks + 2 * 64 * 8;
     }
 };
-
-constexpr int P_WARPS = 4;                     // warps of a CTA that scatter spikes (P) ...
-constexpr int U_THREADS = PT - 32 * P_WARPS;   // ... while the other 896 threads advance neurons (U)
 
 __device__ __forceinline__ void u_sync() { asm volatile("bar.sync 1, %0;" ::"n"(U_THREADS) : "memory"); }
 // barrier of the U threads that also ORs a predicate over them (so every U thread sees the same value)
@@ -165,6 +193,8 @@ __device__ __forceinline__ bool u_sync_or(bool pred)
         : "memory");
     return out != 0;
 }
+__device__ __forceinline__ void push_sync() { asm volatile("bar.sync 2, %0;" ::"n"(PUSH_THREADS) : "memory"); }
+__device__ __forceinline__ void list_sync() { asm volatile("bar.sync 3, %0;" ::"n"(LIST_THREADS) : "memory"); }
 
 // bulk store shared -> global (16-byte aligned, size a multiple of 16), tracked by bulk groups
 __device__ __forceinline__ void tma_store_1d(void* dst_gmem, const void* src_smem, uint32_t bytes)
@@ -175,6 +205,17 @@ __device__ __forceinline__ void tma_store_1d(void* dst_gmem, const void* src_sme
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// The rare inputs of the neuron loop, kept out of line so that the loop body stays small:
+// plastic input arriving at a plastic target, and the steady bias of a biased neuron.
+__device__ __noinline__ float plastic_input(const DevNet& N, const DevState& S, int64_t t, int32_t b, int32_t i)
+{
+    return take_plastic<float>(N, S, t, b, i);
+}
+__device__ __noinline__ float bias_of(const DevState& S, int32_t b, int32_t i)
+{
+    return S.bias_ext[(int64_t)b * S.n_ext + S.ext_idx[i]];
+}
 
 // four consecutive accumulator entries from shared memory (16-byte aligned)
 __device__ __forceinline__ void load4(const int32_t* p, int32_t (&x)[4])
@@ -188,6 +229,130 @@ __device__ __forceinline__ void load4(const int64_t* p, int64_t (&x)[4])
     x[0] = a.x; x[1] = a.y; x[2] = b.x; x[3] = b.y;
 }
 
+// Poisson kicks of step s (tick t) for this CTA's input pairs, OR-ed into `map` (threads tid0, stride).
+// Entries are taken four at a time so that their loads are in flight together.
+template <bool RASTER>
+__device__ __forceinline__ void kicks_into(const DevNet& N, const DevState& S, const PersistArgs& A, uint32_t* map,
+                                           int32_t s, int64_t t, uint32_t step_no, int32_t b0, int32_t G, int64_t lo,
+                                           int32_t e0, int32_t e1, int tid0, int stride, const int64_t* stop)
+{
+    const int32_t n = (int32_t)N.n, np = (int32_t)N.n_pad;
+    constexpr int BATCH = 4;
+    for (int32_t e = e0 + tid0; e < e1; e += BATCH * stride) {
+        int2 en[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; u++) en[u] = (e + u * stride < e1) ? __ldg(A.ext_tab + e + u * stride) : make_int2(0, -1);
+        bool hit[BATCH];
+#pragma unroll
+        for (int u = 0; u < BATCH; u++) {
+            const int32_t k = en[u].x & 0x3ffff, bl = en[u].x >> 18;
+            hit[u] = false;
+            if (en[u].y < 0 || bl >= G || t >= stop[bl]) continue;
+            const int32_t b = b0 + bl;
+            const int32_t i = (int32_t)(lo + k - (int64_t)bl * np);
+            hit[u] = kick_of<RASTER>(S, A.kicks, A.words, N.B, s, b, en[u].y, (uint32_t)((int64_t)b * n + i), step_no);
+        }
+#pragma unroll
+        for (int u = 0; u < BATCH; u++)
+            if (hit[u]) atomicOr(map + ((en[u].x & 0x3ffff) >> 5), 1u << (en[u].x & 31));
+    }
+}
+
+// Exclusive prefix of `x` over the threads tid0 = 0..stride-1 (whole warps) and the total; uses
+// `scratch` (stride / 32 entries of shared memory) and two `sync`s.
+template <typename Sync>
+__device__ __forceinline__ int block_scan(int x, int* total, int32_t* scratch, int tid0, int stride, Sync sync)
+{
+    const int lane = tid0 & 31, warp = tid0 >> 5;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) scratch[warp] = incl;
+    sync();
+    int before = 0, all = 0;
+    for (int w = 0; w < stride / 32; w++) {
+        const int v = scratch[w];
+        before += w < warp ? v : 0;
+        all += v;
+    }
+    sync();
+    *total = all;
+    return before + incl - x;
+}
+
+// One spike of the listing: pair k of this CTA fired at step s (tick t). Counts it, pushes its
+// plastic row, records it, and appends its work items to this CTA's list segment (cursor s_cnt[1]).
+template <bool PLASTIC, bool RECORD>
+__device__ __forceinline__ void list_one(const DevNet& N, const DevState& S, const PersistArgs& A, int2* list, int32_t k,
+                                         int32_t s, int64_t t, int32_t b0, int64_t lo, int32_t* s_cnt)
+{
+    const int32_t np = (int32_t)N.n_pad;
+    const int64_t lp = lo + k;
+    const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
+    const int32_t b = b0 + bl;
+    red_add(A.counts + (int64_t)b * N.n + i, 1);
+    const int nch = (int)((__ldg(N.rowptr + i + 1) - __ldg(N.rowptr + i) + CHUNK - 1) / CHUNK);
+    if (PLASTIC) push_plastic_row(N, S, t, b, i);
+    if (RECORD) {
+        if (A.step_counts) atomicAdd(A.step_counts + (int64_t)s * N.B + b, 1);
+        if (A.step_digest)
+            atomicAdd(reinterpret_cast<unsigned long long*>(A.step_digest + (int64_t)s * N.B + b),
+                      (unsigned long long)spike_tag((uint64_t)i));
+    }
+    if (nch == 0) return;
+    int base = atomicAdd(&s_cnt[1], nch);
+    for (int c = 0; c < nch; c++, base++) {
+        if (base < S.cap_c) list[base] = make_item(N, i, b, c);
+        else atomicExch(S.err, 1);
+    }
+}
+
+// The spikes of step s (tick t) recorded in `map`: counts, plastic rows, records, and the work items
+// of this CTA's segment of the group's list; the segment's count is stored at the end. Clears `map`.
+// The spikes are first gathered into `spk` (SPK_BUF entries) so that each is then handled by its
+// own thread, their memory accesses all in flight at once; spikes beyond the buffer are handled
+// where they are found. Threads tid0 = 0..stride-1 (whole warps) all call it (synchronised by `sync`).
+template <bool PLASTIC, bool RECORD, typename Sync>
+__device__ __forceinline__ void list_spikes(const DevNet& N, const DevState& S, const PersistArgs& A, uint32_t* map,
+                                            int32_t s, int64_t t, int32_t b0, int32_t q, int64_t lo, int32_t used_words,
+                                            int32_t* s_cnt, int32_t* scratch, int32_t* spk, int tid0, int stride,
+                                            Sync sync)
+{
+    const int64_t slot = pos_mod(t, N.R);
+    int2* list = list_of(S, slot, q, blockIdx.x);
+    const int32_t wpt = (used_words + stride - 1) / stride;      // contiguous words per thread
+    const int32_t wa = min(tid0 * wpt, used_words), wb = min(wa + wpt, used_words);
+    int mine = 0;
+    for (int32_t w = wa; w < wb; w++) mine += __popc(map[w]);
+    int total = 0;
+    int pos = block_scan(mine, &total, scratch, tid0, stride, sync);
+    if (mine) {
+        for (int32_t w = wa; w < wb; w++) {
+            uint32_t m = map[w];
+            if (!m) continue;
+            map[w] = 0u;
+            for (; m; m &= m - 1, pos++) {
+                const int32_t k = w * 32 + __ffs(m) - 1;
+                if (pos < SPK_BUF) spk[pos] = k;
+                else list_one<PLASTIC, RECORD>(N, S, A, list, k, s, t, b0, lo, s_cnt);
+            }
+        }
+    }
+    sync();
+    for (int j = tid0; j < min(total, SPK_BUF); j += stride)
+        list_one<PLASTIC, RECORD>(N, S, A, list, spk[j], s, t, b0, lo, s_cnt);
+    sync();
+    if (tid0 == 0) {
+        *count_of(S, slot, q, blockIdx.x) = s_cnt[1];
+        s_cnt[1] = 0;
+    }
+}
+
+// One launch runs `A.steps` steps of the instances [b0, b0 + G) (group q); the warp roles and the
+// bitmap rotation are described at the top of this file.
 template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD, int LANES>
 __global__ void __launch_bounds__(PT, 1)
     k_persist(const DevNet N, const DevState S, const PersistArgs A, int32_t b0, int32_t G, int32_t q, int64_t per)
@@ -199,14 +364,19 @@ __global__ void __launch_bounds__(PT, 1)
     AccT* sacc = reinterpret_cast<AccT*>(smem + lay.acc);
     float* sv = reinterpret_cast<float*>(smem + lay.v);
     float* sg = reinterpret_cast<float*>(smem + lay.g);
-    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + lay.kbits);  // kicks before U, spikes after
+    uint32_t* maps = reinterpret_cast<uint32_t*>(smem + lay.kbits);
     uint8_t* sr = smem + lay.ref;            // bits 0-5 refractory, 6 plastic target, 7 nonzero bias
     uint8_t* s_active = smem + lay.misc;
-    int32_t* s_cnt = reinterpret_cast<int32_t*>(smem + lay.misc + 64);   // total, cursor, base
-    const Lif<float>& L = N.L32;
+    int32_t* s_cnt = reinterpret_cast<int32_t*>(smem + lay.misc + 64);   // -, list cursor, push totals x2
+    int32_t* s_scan = reinterpret_cast<int32_t*>(smem + lay.scan);
+    int32_t* s_pre = reinterpret_cast<int32_t*>(smem + lay.pre);         // segment prefixes x2 (step parity)
+    int32_t* s_spk = reinterpret_cast<int32_t*>(smem + lay.spk);
+    int64_t* s_reset = reinterpret_cast<int64_t*>(smem + lay.ticks);     // per instance of the group
+    int64_t* s_stop = s_reset + 64;
+    const Lif<float> L = N.L32;
+    const int n_ref = N.n_ref;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
-    const bool u_warp = tid < U_THREADS;
     const int32_t n = (int32_t)N.n, np = (int32_t)N.n_pad;
     const int64_t lo = (int64_t)blockIdx.x * per;
     const int32_t cnt = (int32_t)max((int64_t)0, min(per, (int64_t)G * np - lo));
@@ -214,7 +384,7 @@ __global__ void __launch_bounds__(PT, 1)
     float* V = reinterpret_cast<float*>(S.v);
     float* Gs = reinterpret_cast<float*>(S.g);
     const int32_t e0 = A.ext_off[blockIdx.x], e1 = A.ext_off[blockIdx.x + 1];
-    const int32_t nwords = (int32_t)((per + 4 * PT) / 32 + 1);
+    const int32_t wpm = (int32_t)lay.words_per_map;
     const int32_t used_words = (cnt + 31) / 32;
 
     // ---- load this CTA's state into shared memory ------------------------------------------
@@ -231,12 +401,17 @@ __global__ void __launch_bounds__(PT, 1)
         }
         sr[k] = f;
     }
-    for (int32_t w = tid; w < nwords; w += PT) kbits[w] = 0u;
+    for (int32_t w = tid; w < 3 * wpm; w += PT) maps[w] = 0u;
     for (int32_t z = tid; z < ZERO_PAGE / 4; z += PT) reinterpret_cast<uint32_t*>(smem + lay.zero)[z] = 0u;
     fence_proxy_async_shared();                                  // zero page visible to bulk copies
     if (tid == 0) {
         mbar_init(mbar, 1);
         fence_mbar_init();
+        for (int c = 0; c < 8; c++) s_cnt[c] = 0;
+    }
+    if (tid < G) {                                               // the ticks stay constant during a launch
+        s_reset[tid] = S.reset_tick[b0 + tid];
+        s_stop[tid] = S.stop_tick[b0 + tid];
     }
     __syncthreads();
     for (int32_t e = e0 + tid; e < e1; e += PT) {               // bias is constant during a launch
@@ -244,20 +419,21 @@ __global__ void __launch_bounds__(PT, 1)
         const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
         if (bl < G && S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + en.y] != 0.0f) sr[k] |= 0x80;
     }
+    if (A.steps > 0) kicks_into<RASTER>(N, S, A, maps, 0, A.t0, A.step0, b0, G, lo, e0, e1, tid, PT, s_stop);
     __syncthreads();
 
     unsigned int barriers = 0;
     int32_t* err = S.err;
     const uint32_t acc_bytes = (uint32_t)cnt * (uint32_t)sizeof(AccT);
     const int32_t i0 = (int32_t)((lo + 4 * tid) % np), bl0 = (int32_t)((lo + 4 * tid) / np);
-    const int64_t p_tid = (int64_t)blockIdx.x * (PT - U_THREADS) + (tid - U_THREADS);
-    const int64_t p_threads = (int64_t)gridDim.x * (PT - U_THREADS);
+    int32_t last = -1;                                          // step whose spikes still need listing
 
     for (int32_t s = 0; s < A.steps; s++) {
         const int64_t t = A.t0 + s;
         const uint32_t step_no = A.step0 + (uint32_t)s;
         const AccT* acc = reinterpret_cast<const AccT*>((t & 1) ? S.acc1 : S.acc0);
-        const int64_t slot = pos_mod(t, N.R);
+        uint32_t* map = maps + (s % 3) * wpm;
+        if (tid == 0) stamp(A, s, 0);
         // the accumulator slice of this step -> shared memory, one bulk load
         if (tid == 0 && cnt > 0) {
             fence_proxy_async_global();
@@ -267,42 +443,32 @@ __global__ void __launch_bounds__(PT, 1)
                             reinterpret_cast<const uint8_t*>(acc + acc_base) + off, min((uint32_t)LOAD_PIECE, acc_bytes - off),
                             mbar);
         }
-        if (tid < G) s_active[tid] = t < S.stop_tick[b0 + tid];
-        if (tid == 32) s_cnt[0] = s_cnt[1] = 0;
-        if (blockIdx.x == 0 && tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q) = 0;
+        if (tid < G) s_active[tid] = t < s_stop[tid];
+        // this CTA's segment consumed by the pushes at t-1 starts empty (the step engine appends to it)
+        if (tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q, blockIdx.x) = 0;
         __syncthreads();
-        if (u_warp) {
-            // ---- U1: Poisson kicks of the input pairs into the bitmap (overlaps the load) ----------
-            for (int32_t e = e0 + tid; e < e1; e += U_THREADS) {
-                const int2 en = __ldg(A.ext_tab + e);
-                const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
-                if (bl >= G || !s_active[bl]) continue;
-                const int32_t b = b0 + bl;
-                const int32_t i = (int32_t)(lo + k - (int64_t)bl * np);
-                if (kick_of<RASTER>(S, A.kicks, A.words, N.B, s, b, en.y, (uint32_t)((int64_t)b * n + i), step_no))
-                    atomicOr(kbits + (k >> 5), 1u << (k & 31));
-            }
-            u_sync();
+        if (tid < U_THREADS) {
+            if (tid == 0) stamp(A, s, 1);
             bool ok = true;
             if (cnt > 0 && tid == 0) ok = stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
             ok = !u_sync_or(!ok);        // one thread waited; every U thread agrees on the outcome
             if (cnt > 0 && ok) (void)mbar_try_wait(mbar, (uint32_t)(s & 1));   // completed: acquire only
-            if (cnt > 0) {
-                if (tid == 0 && ok) {    // the slice is in shared memory: clear it in global memory
-                    AccT* accw = const_cast<AccT*>(acc) + acc_base;
-                    for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
-                        tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
-                    bulk_commit();
-                }
+            if (tid == 0) stamp(A, s, 2);
+            if (cnt > 0 && ok && tid == 0) {     // the slice is in shared memory: clear it in global memory
+                AccT* accw = const_cast<AccT*>(acc) + acc_base;
+                for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
+                    tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
+                bulk_commit();
             }
-            // ---- U2: advance every owned pair, four consecutive pairs per thread (a quad never
-            //      straddles two instances: rows are padded to 16); a spike only sets its bit ---------
+            // ---- advance every owned pair, four consecutive pairs per thread (a quad never straddles
+            //      two instances: rows are padded to 16); the step's kicks are read from the map and
+            //      its spikes written back into it --------------------------------------------------
             if (ok) {
                 int32_t i = i0, bl = bl0;
                 const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
                 for (int32_t kb = 0; kb < cnt; kb += 4 * U_THREADS) {
                     const int32_t k = kb + 4 * tid;
-                    const uint32_t kick4 = (kbits[k >> 5] >> sh) & 15u;
+                    const uint32_t kick4 = (map[k >> 5] >> sh) & 15u;
                     uint32_t spk4 = 0;
                     if (k < cnt && i < n && s_active[bl]) {
                         AccT x[4];
@@ -317,11 +483,12 @@ __global__ void __launch_bounds__(PT, 1)
                             if (i + j >= n) continue;
                             float buf = acc_to_real<float>(x[j], L.w_syn);
                             const uint32_t f = ff[j];
-                            if (PLASTIC && (f & 0x40)) buf = add_rn(buf, take_plastic<float>(N, S, t, b0 + bl, i + j));
+                            if (PLASTIC && (f & 0x40)) buf = add_rn(buf, plastic_input(N, S, t, b0 + bl, i + j));
                             int r = (int)(f & 0x3f);
                             const bool hb = (f & 0x80) != 0;
-                            const float bias = hb ? S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + S.ext_idx[i + j]] : 0.0f;
-                            if (lif_step<float>(vv[j], gg[j], r, buf, hb, bias, (kick4 >> j) & 1u, L, N.n_ref, N.contract != 0))
+                            const float bias = hb ? bias_of(S, b0 + bl, i + j) : 0.0f;
+                            // the engine always fuses the two multiply-adds, as the shipped reference does
+                            if (lif_step<float>(vv[j], gg[j], r, buf, hb, bias, (kick4 >> j) & 1u, L, n_ref, true))
                                 spk4 |= 1u << j;
                             ff[j] = (f & 0xc0) | (uint32_t)r;
                         }
@@ -335,80 +502,67 @@ __global__ void __launch_bounds__(PT, 1)
                     word |= __shfl_xor_sync(0xffffffffu, word, 1);
                     word |= __shfl_xor_sync(0xffffffffu, word, 2);
                     word |= __shfl_xor_sync(0xffffffffu, word, 4);
-                    if ((lane & 7) == 0) kbits[k >> 5] = word;
+                    if ((lane & 7) == 0) map[k >> 5] = word;
                     i += 4 * U_THREADS;
                     while (i >= np) { i -= np; bl++; }
                 }
             }
-            u_sync();
-            // ---- U3: this step's spikes: counts, plastic rows, work items (one atomic per CTA) ----
-            int my_items = 0;
-            for (int32_t w = tid; w < used_words && ok; w += U_THREADS) {
-                uint32_t m = kbits[w];
-                while (m) {
-                    const int32_t k = w * 32 + __ffs(m) - 1;
-                    m &= m - 1;
-                    const int64_t lp = lo + k;
-                    const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
-                    const int32_t b = b0 + bl;
-                    A.counts[(int64_t)b * n + i] += 1;
-                    my_items += (int)((N.rowptr[i + 1] - N.rowptr[i] + CHUNK - 1) / CHUNK);
-                    if (PLASTIC) push_plastic_row(N, S, t, b, i);
-                    if (RECORD) {
-                        if (A.step_counts) atomicAdd(A.step_counts + (int64_t)s * N.B + b, 1);
-                        if (A.step_digest)
-                            atomicAdd(reinterpret_cast<unsigned long long*>(A.step_digest + (int64_t)s * N.B + b),
-                                      (unsigned long long)spike_tag((uint64_t)i));
-                    }
-                }
-            }
-            if (my_items) atomicAdd(&s_cnt[0], my_items);
-            u_sync();
-            if (tid == 0 && s_cnt[0] > 0) s_cnt[2] = atomicAdd(count_of(S, slot, q), s_cnt[0]);
-            u_sync();
-            {   // second pass: write the items, and clear every word for the next step's kicks
-                int2* list = list_of(S, slot, q);
-                for (int32_t w = tid; w < used_words; w += U_THREADS) {
-                    uint32_t m = kbits[w];
-                    if (!m) continue;
-                    kbits[w] = 0u;
-                    while (m && ok) {
-                        const int32_t k = w * 32 + __ffs(m) - 1;
-                        m &= m - 1;
-                        const int64_t lp = lo + k;
-                        const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
-                        const int nch = (int)((N.rowptr[i + 1] - N.rowptr[i] + CHUNK - 1) / CHUNK);
-                        if (nch == 0) continue;
-                        const int64_t p0 = (int64_t)s_cnt[2] + atomicAdd(&s_cnt[1], nch);
-                        for (int c = 0; c < nch; c++) {
-                            if (p0 + c < S.cap_g) list[p0 + c] = make_item(N, i, b0 + bl, c);
-                            else atomicExch(err, 1);
-                        }
-                    }
-                }
-            }
             fence_proxy_async_shared();          // reads of the slice before the next bulk load
-        } else {
-            // ---- P: scatter the spikes that arrive at t+1 into the other accumulator ---------------
-            if (N.n_delay > 1) {
-                AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
-                push_list<AccT, LANES>(N, S, t, q, acc_next, p_tid, p_threads);
-            }
-        }
-        if (N.n_delay == 1) {                // P needs this step's spikes: after a grid barrier
-            barriers++;
-            if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) break;
+            if (tid == 0) stamp(A, s, 3);
+            // ---- the next step's kicks (they depend on nothing this step computes) ----------------
+            if (s + 1 < A.steps)
+                kicks_into<RASTER>(N, S, A, maps + ((s + 1) % 3) * wpm, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1,
+                                   tid, U_THREADS, s_stop);
+            if (tid == 0) stamp(A, s, 4);
+        } else if (tid < U_THREADS + PUSH_THREADS) {
+            const int ptid = tid - U_THREADS;
+            if (ptid == 0) stamp(A, s, 7);
+            // ---- scatter the items that arrive at t+1 into the other accumulator -------------------
             AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
-            push_list<AccT, LANES>(N, S, t, q, acc_next, (int64_t)blockIdx.x * PT + tid, (int64_t)gridDim.x * PT);
+            int32_t* pre = s_pre + (s & 1) * MAX_SEG;
+            if (t + 1 - N.n_delay >= 0) {
+                // the segment prefix of the list scattered now; with n_delay >= 4 the previous step
+                // computed it already (its counts were final one barrier earlier)
+                if (ptid < 32 && (s == 0 || N.n_delay < 4)) {
+                    const int32_t tot = segment_prefix(S, pos_mod(t + 1 - N.n_delay, N.R), q, pre);
+                    if (ptid == 0) s_cnt[2 + (s & 1)] = tot;
+                }
+                push_sync();
+                if (ptid == 0) stamp(A, s, 9);
+                const int64_t total = s_cnt[2 + (s & 1)];   // this CTA's share: a contiguous range of items
+                const int64_t g0 = total * blockIdx.x / gridDim.x, g1 = total * (blockIdx.x + 1) / gridDim.x;
+                push_range<AccT, LANES>(N, S, t, q, acc_next, pre, g0, g1, ptid / LANES, PUSH_THREADS / LANES,
+                                        ptid % LANES, s_reset, s_stop, b0);
+            }
+            // ---- the next step's segment prefix (its counts were written before this step began)
+            if (N.n_delay >= 4 && ptid < 32 && t + 2 - N.n_delay >= 0) {
+                const int32_t tot = segment_prefix(S, pos_mod(t + 2 - N.n_delay, N.R), q, s_pre + ((s + 1) & 1) * MAX_SEG);
+                if (ptid == 0) s_cnt[2 + ((s + 1) & 1)] = tot;
+            }
+            if (ptid == 0) stamp(A, s, 10);
+        } else {
+            // ---- the previous step's spikes: counts, plastic rows, work items ---------------------
+            const int lt = tid - U_THREADS - PUSH_THREADS;
+            if (s >= 1)
+                list_spikes<PLASTIC, RECORD>(N, S, A, maps + ((s - 1) % 3) * wpm, s - 1, t - 1, b0, q, lo, used_words,
+                                             s_cnt, s_scan, s_spk, lt, LIST_THREADS, []() { list_sync(); });
+            if (lt == 0) stamp(A, s, 8);
         }
         if (tid == 0 && cnt > 0) {
             bulk_wait_all();                     // the cleared slice is written before anyone pushes into it
             fence_proxy_async_global();
         }
+        if (tid == 0) stamp(A, s, 5);
         barriers++;
-        if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) break;
+        last = s;
+        if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) { last = -1; break; }
+        if (tid == 0) stamp(A, s, 6);
     }
     if (tid == 0) bulk_wait_all();
+    // the last step's spikes are listed before the launch ends (the next launch scatters them)
+    if (last >= 0)
+        list_spikes<PLASTIC, RECORD>(N, S, A, maps + (last % 3) * wpm, last, A.t0 + last, b0, q, lo, used_words, s_cnt,
+                                     s_scan, s_spk, tid, PT, []() { __syncthreads(); });
 
     // ---- write the state back ------------------------------------------------------------------
     __syncthreads();
@@ -425,11 +579,11 @@ __global__ void __launch_bounds__(PT, 1)
 }
 
 // Largest group whose state fits in shared memory of `ctas` CTAs; 0 if not even one instance does.
-inline PersistPlan plan_persistent(int64_t n, int64_t n_pad, int32_t B, bool f64, int n_ref, int acc_bytes,
-                                   int sm_count, int device)
+inline PersistPlan plan_persistent(int64_t n, int64_t n_pad, int32_t B, bool f64, int n_ref, int n_delay,
+                                   int acc_bytes, int sm_count, int device)
 {
     PersistPlan P{};
-    if (f64 || n_ref > 63) return P;
+    if (f64 || n_ref > 63 || n_delay < 3) return P;
     int smem_optin = 0;
     cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     if (smem_optin <= 0) smem_optin = 232448;
@@ -448,7 +602,7 @@ inline PersistPlan plan_persistent(int64_t n, int64_t n_pad, int32_t B, bool f64
     const int32_t G = (B + n_groups - 1) / n_groups;
     int64_t per = ((int64_t)G * n_pad + ctas - 1) / ctas;
     per = (per + 15) / 16 * 16;
-    if (per > per_max || per >= ((int64_t)1 << 18)) return P;
+    if (per > per_max || per >= ((int64_t)1 << 18) || ctas > MAX_SEG) return P;
     P.group = G;
     P.n_groups = n_groups;
     P.ctas = ctas;

@@ -68,7 +68,7 @@ typedef struct {
     int64_t t;            /* simulated steps since the last full reset (BatchBrain.t) */
     uint32_t step_no;     /* global step counter feeding the Poisson hash (BatchBrain.step_no) */
     int64_t launches;     /* kernels launched by this engine so far */
-    int64_t item_capacity;/* spike work items per (step, instance group) list */
+    int64_t item_capacity;/* spike work items per (step, instance group, list segment) list */
     int64_t bytes_device; /* device memory held by the engine */
     double decay_syn;     /* exp(-dt / tau_syn), computed in FP64 on the device */
     double decay_m;       /* dt / tau_m */
@@ -157,6 +157,13 @@ int fb_reward_step(fb_brain* brain, const int32_t* counts, double* elig, float* 
 
 /* Choose the schedule (FB_ENGINE_*, FB_PROP_*, lanes per work item 8/16/32; 0 keeps a field). */
 int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
+
+/* Phase trace of the persistent engine (diagnostics). `trace` [device] holds `capacity` int64;
+ * every later fb_run whose steps * ctas * 11 fits records, per step and CTA, the SM clock at 11
+ * points: step start, neuron warps start, accumulator slice staged, neurons advanced, next kicks
+ * done, barrier arrival (neuron warps), barrier exit, push warps start, listing warps done, push
+ * warps' segment prefix ready, push warps done. NULL: off. No counterpart in the reference. */
+int fb_set_trace(fb_brain* brain, long long* trace, int64_t capacity);
 
 /* Device error flags raised since the last call (overflow, barrier timeout), then cleared.
  * Synchronises `stream`. Returns FB_OK or the first raised FB_ERR_* code. */

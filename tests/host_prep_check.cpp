@@ -85,6 +85,23 @@ int main()
             }
         }
         CHECK(chunks == H.chunks_all);
+        // segment capacity: brute force over the pairs of a group of 1..3 instances
+        {
+            const int64_t n_pad = (n + 15) / 16 * 16;
+            const int64_t group = 1 + trial % 3, pairs = group * n_pad;
+            const int64_t n_seg = 1 + (int64_t)(g() % 9);
+            const int64_t seg_pairs = ((pairs + n_seg - 1) / n_seg + 15) / 16 * 16;
+            int64_t want = 1;
+            for (int64_t s = 0; s < n_seg; s++) {
+                int64_t items = 0;
+                for (int64_t p = s * seg_pairs; p < std::min((s + 1) * seg_pairs, pairs); p++) {
+                    const int64_t i = p % n_pad;
+                    if (i < n) items += (H.rp[i + 1] - H.rp[i] + 255) / 256;
+                }
+                want = std::max(want, items);
+            }
+            CHECK(segment_capacity(H, n_pad, group, seg_pairs, n_seg) == want);
+        }
 
         // plastic plans: a random subset, then a superset; weights and ring survive the re-plan
         if (nnz == 0) continue;
