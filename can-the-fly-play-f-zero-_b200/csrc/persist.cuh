@@ -9,9 +9,9 @@
 // reductions they scatter.
 //
 // Warp roles of a CTA (all steps, separated by one grid barrier per step):
-//   neuron warps (U, 28): stage the slice, advance every owned pair, then draw the next step's
+//   neuron warps (U, 26): stage the slice, advance every owned pair, then draw the next step's
 //     Poisson kicks into a shared bitmap;
-//   push warps (2): scatter the work items that arrive next step into the other accumulator;
+//   push warps (4): scatter the work items that arrive next step into the other accumulator;
 //   listing warps (2): list the previous step's spikes (counts, plastic rows, work items of this
 //     CTA's segment of the group's list).
 // A spike of step s is listed during step s+1 and first scattered during step s+n_delay-1, so
@@ -30,7 +30,7 @@ constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulato
 constexpr int SPK_BUF = 1024;           // spikes of one CTA and step listed in parallel
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
 
-constexpr int PUSH_WARPS = 2;                              // warps that scatter arriving items ...
+constexpr int PUSH_WARPS = 4;                              // warps that scatter arriving items ...
 constexpr int LIST_WARPS = 2;                              // ... that list the previous step's spikes ...
 constexpr int PUSH_THREADS = 32 * PUSH_WARPS;
 constexpr int LIST_THREADS = 32 * LIST_WARPS;
@@ -206,15 +206,37 @@ __device__ __forceinline__ void tma_store_1d(void* dst_gmem, const void* src_sme
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
-// The rare inputs of the neuron loop, kept out of line so that the loop body stays small:
-// plastic input arriving at a plastic target, and the steady bias of a biased neuron.
-__device__ __noinline__ float plastic_input(const DevNet& N, const DevState& S, int64_t t, int32_t b, int32_t i)
+// A quad of the neuron loop with a plastic target or a biased neuron among its pairs, kept out of
+// line so that the common loop body stays small. Advances pairs 0..nvalid-1 of the quad in
+// shared memory (xs, vs, gs, fs) and returns their spike bits. Plastic input arriving at a target
+// is read from pring_row[ppost_of_i[j]] and cleared (L2 only: other SMs pushed it); a biased
+// pair's bias is bias_row[ext_idx_i[j]].
+template <typename AccT, bool PLASTIC>
+__device__ __noinline__ uint32_t quad_special(const AccT* xs, float* vs, float* gs, uint8_t* fs, uint32_t kick4,
+                                              int nvalid, int64_t* pring_row, const int32_t* ppost_of_i,
+                                              const float* bias_row, const int32_t* ext_idx_i, const Lif<float> L,
+                                              int n_ref)
 {
-    return take_plastic<float>(N, S, t, b, i);
-}
-__device__ __noinline__ float bias_of(const DevState& S, int32_t b, int32_t i)
-{
-    return S.bias_ext[(int64_t)b * S.n_ext + S.ext_idx[i]];
+    uint32_t spk4 = 0;
+    for (int j = 0; j < nvalid; j++) {
+        float buf = acc_to_real<float>(xs[j], L.w_syn);
+        const uint32_t f = fs[j];
+        if (PLASTIC && (f & 0x40)) {
+            int64_t* q = pring_row + ppost_of_i[j];
+            const int64_t px = __ldcg(reinterpret_cast<const long long*>(q));
+            if (px != 0) *q = 0;
+            buf = add_rn(buf, from_q32<float>(px));
+        }
+        int r = (int)(f & 0x3f);
+        const bool hb = (f & 0x80) != 0;
+        const float bias = hb ? bias_row[ext_idx_i[j]] : 0.0f;
+        float v = vs[j], g = gs[j];
+        if (lif_step<float>(v, g, r, buf, hb, bias, (kick4 >> j) & 1u, L, n_ref, true)) spk4 |= 1u << j;
+        vs[j] = v;
+        gs[j] = g;
+        fs[j] = (uint8_t)((f & 0xc0) | (uint32_t)r);
+    }
+    return spk4;
 }
 
 // four consecutive accumulator entries from shared memory (16-byte aligned)
@@ -471,31 +493,35 @@ __global__ void __launch_bounds__(PT, 1)
                     const uint32_t kick4 = (map[k >> 5] >> sh) & 15u;
                     uint32_t spk4 = 0;
                     if (k < cnt && i < n && s_active[bl]) {
-                        AccT x[4];
-                        load4(sacc + k, x);
-                        const float4 v4 = *reinterpret_cast<const float4*>(sv + k);
-                        const float4 g4 = *reinterpret_cast<const float4*>(sg + k);
-                        const uchar4 f4 = *reinterpret_cast<const uchar4*>(sr + k);
-                        float vv[4] = {v4.x, v4.y, v4.z, v4.w}, gg[4] = {g4.x, g4.y, g4.z, g4.w};
-                        uint32_t ff[4] = {f4.x, f4.y, f4.z, f4.w};
+                        const uint32_t fl = *reinterpret_cast<const uint32_t*>(sr + k);
+                        if ((fl & 0xc0c0c0c0u) == 0) {   // no plastic target, no bias: the common quad
+                            AccT x[4];
+                            load4(sacc + k, x);
+                            const float4 v4 = *reinterpret_cast<const float4*>(sv + k);
+                            const float4 g4 = *reinterpret_cast<const float4*>(sg + k);
+                            float vv[4] = {v4.x, v4.y, v4.z, v4.w}, gg[4] = {g4.x, g4.y, g4.z, g4.w};
+                            uint32_t ff = fl;
 #pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            if (i + j >= n) continue;
-                            float buf = acc_to_real<float>(x[j], L.w_syn);
-                            const uint32_t f = ff[j];
-                            if (PLASTIC && (f & 0x40)) buf = add_rn(buf, plastic_input(N, S, t, b0 + bl, i + j));
-                            int r = (int)(f & 0x3f);
-                            const bool hb = (f & 0x80) != 0;
-                            const float bias = hb ? bias_of(S, b0 + bl, i + j) : 0.0f;
-                            // the engine always fuses the two multiply-adds, as the shipped reference does
-                            if (lif_step<float>(vv[j], gg[j], r, buf, hb, bias, (kick4 >> j) & 1u, L, n_ref, true))
-                                spk4 |= 1u << j;
-                            ff[j] = (f & 0xc0) | (uint32_t)r;
+                            for (int j = 0; j < 4; j++) {
+                                if (i + j >= n) continue;
+                                int r = (int)((fl >> (8 * j)) & 0x3f);
+                                // the engine always fuses the two multiply-adds, as the shipped reference does
+                                if (lif_step<float>(vv[j], gg[j], r, acc_to_real<float>(x[j], L.w_syn), false, 0.0f,
+                                                    (kick4 >> j) & 1u, L, n_ref, true))
+                                    spk4 |= 1u << j;
+                                ff = (ff & ~(0xffu << (8 * j))) | ((uint32_t)r << (8 * j));
+                            }
+                            *reinterpret_cast<float4*>(sv + k) = make_float4(vv[0], vv[1], vv[2], vv[3]);
+                            *reinterpret_cast<float4*>(sg + k) = make_float4(gg[0], gg[1], gg[2], gg[3]);
+                            *reinterpret_cast<uint32_t*>(sr + k) = ff;
+                        } else {
+                            const int32_t b = b0 + bl;
+                            int64_t* pring_row =
+                                PLASTIC ? S.pring + (pos_mod(t, N.R) * N.B + b) * (int64_t)N.n_ppost : nullptr;
+                            spk4 = quad_special<AccT, PLASTIC>(sacc + k, sv + k, sg + k, sr + k, kick4, min(4, n - i),
+                                                               pring_row, N.ppost_of + i,
+                                                               S.bias_ext + (int64_t)b * S.n_ext, S.ext_idx + i, L, n_ref);
                         }
-                        *reinterpret_cast<float4*>(sv + k) = make_float4(vv[0], vv[1], vv[2], vv[3]);
-                        *reinterpret_cast<float4*>(sg + k) = make_float4(gg[0], gg[1], gg[2], gg[3]);
-                        *reinterpret_cast<uchar4*>(sr + k) =
-                            make_uchar4((uint8_t)ff[0], (uint8_t)ff[1], (uint8_t)ff[2], (uint8_t)ff[3]);
                     }
                     // the 8 lanes of a 32-pair word OR their nibbles together; one of them stores it
                     uint32_t word = spk4 << sh;

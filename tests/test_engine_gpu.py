@@ -335,3 +335,38 @@ def test_device_decay_factors_match_numpy(torch):
         assert b.decay_syn == np.float32(np.exp(-dt / p.tau_syn))
         assert b.decay_m == np.float32(dt / p.tau_m)
         assert b.kick == np.float32(p.f_poisson * p.w_syn)
+
+
+@pytest.mark.parametrize("dt", [0.6, 0.45, 0.36])
+def test_persistent_short_delays_bias_and_plastic(torch, dt):
+    """The persistent engine at its shortest delays (n_delay 3, 4, 5: spikes listed one step late,
+    pushed n_delay-1 steps later), with biased neurons and plastic targets on the out-of-line path,
+    over chained launches: bit-exact vs the oracle."""
+    from flyzero_b200.brain import LIFParams
+
+    conn = cx.synthetic(4096, seed=7)
+    B = 3
+    rng = np.random.default_rng(11)
+    pos = np.sort(rng.choice(conn.weights.nnz, 300, replace=False))
+    gb = _bb(conn.weights, LIFParams(dt=dt), B, "persistent", plastic_pos=pos, seed=6)
+    assert gb.info().n_delay == int(round(1.8 / dt))
+    eo = O.EngineOracle(conn.weights, O.Params(dt=dt), batch=B, plastic_pos=pos, seed=6)
+    idx, rate = wl.config1_inputs(conn.n, seed=7)
+    gb.set_input(idx, rate * 3)
+    j = eo.slots(idx)
+    eo.p_ext[:, j] = (rate * 3) * np.float32(dt / 1000.0)
+    bidx = rng.choice(conn.n, 50, replace=False)
+    mv = rng.uniform(0, 8, (B, 50)).astype(np.float32)
+    gb.set_bias(bidx, mv)
+    jb = eo.slots(bidx)              # (grows the oracle's ext arrays)
+    eo.bias_ext[:, jb] = mv
+    scale = rng.uniform(0.5, 2.0, (B, len(pos))).astype(np.float32)
+    gb.pw *= torch.as_tensor(scale, device=gb.device)
+    eo.pw[:] = gb.pw.cpu().numpy()
+    total = 0
+    for steps in (40, 25, 60):
+        c = gb.run_steps(steps).cpu().numpy()
+        np.testing.assert_array_equal(c, eo.run_steps(steps))
+        total += c.sum()
+    _compare_state(torch, gb, eo)
+    assert total > 0
