@@ -1,0 +1,42 @@
+"""Precision report (FP32 state + exact INT32 accumulation vs the FP64 oracle-mode engine) on the
+high-activity workload, small size: the report is consistent and the FP32 engine tracks FP64."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def test_precision_report_high_activity(torch):
+    from flyzero_b200 import connectome as cx
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+    from flyzero_b200.precision import precision_report
+
+    conn = cx.synthetic(8192, seed=3)
+    idx, rate = wl.high_activity_inputs(conn.n, seed=3)
+    steps, B = 1500, 3
+    rep = precision_report(conn.weights, LIFParams(dt=0.1), B, idx, rate, steps, seed=4)
+    assert rep["spikes_per_step_fp64"] > 3              # high activity: spikes every step
+    for inst in rep["instances"]:
+        assert 0 < inst["horizon_steps"] <= steps
+        # while the rasters agree, FP32 state stays within a small distance of FP64
+        assert inst["max_dv_mv_before_horizon"] < 1e-3
+        assert inst["mean_rate_hz_fp64"] > 5
+    # the FP64 half of the report is the FP64 engine's own run
+    b64 = BatchBrain(conn.weights, LIFParams(dt=0.1), batch=B, seed=4, fp64=True)
+    b64.set_input(idx, rate)
+    c = b64.run_steps(steps).cpu().numpy()
+    secs = steps * 0.1 / 1000.0
+    got = [x["mean_rate_hz_fp64"] for x in rep["instances"]]
+    np.testing.assert_allclose(got, c.mean(1) / secs, rtol=1e-12)
