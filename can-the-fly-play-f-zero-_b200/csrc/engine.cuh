@@ -13,7 +13,9 @@
 //               to 16 entries so that every row starts on a 64-byte boundary (TMA bulk copies);
 //               items[R][n_groups][n_seg][cap_c] int2: spike work lists of the last R = n_delay+1
 //               steps, one per instance group and segment (the pairs one persistent CTA owns);
-//               item_count[R][n_groups][n_seg]; pring[R][B][n_ppost] i64: plastic input
+//               item_count[R][n_groups][n_seg]; pring[R][B][n_ppost] i64: plastic input;
+//               with pull propagation also masks[R][n][ceil(B/64)] u64: which instances each
+//               neuron spiked in, and the connectome by postsynaptic neuron (colptr, cpre, ccnt/cwfx)
 //
 // The delay line is "deferred push": the fixed-weight rows of the spikes of step s are scattered
 // into acc only at step s + n_delay - 1, right before they arrive, so only two accumulator slots
@@ -38,6 +40,10 @@ struct DevNet {
     const int32_t* pl_pidx;
     const int64_t* pl_q0;      // q32 of each plastic entry's connectome weight
     const int32_t* ppost_of;
+    const int64_t* colptr;     // pull propagation: the connectome by postsynaptic neuron (or nullptr)
+    const int32_t* cpre;
+    const int16_t* ccnt;
+    const int64_t* cwfx;
     Lif<float> L32;
     Lif<double> L64;
 };
@@ -63,6 +69,8 @@ struct DevState {
     int64_t seg_pairs;         // pairs per segment; pair (b, i) = (b mod group) * n_pad + i
     const int64_t* reset_tick;
     const int64_t* stop_tick;
+    unsigned long long* masks; // pull propagation: [R][n][mask_words] spiking instances per neuron (or nullptr)
+    int32_t mask_words;        // ceil(B / 64)
     int32_t* err;              // [0] overflow, [1] barrier timeout step (host-mapped)
     uint32_t seed;
 };
@@ -253,6 +261,8 @@ __global__ void __launch_bounds__(256) k_update(const DevNet N, const DevState S
                 if (r != r0) S.ref[pair] = (int8_t)r;
                 if (spk) {
                     A.counts[pair] += 1;
+                    if (S.masks)
+                        atomicOr(S.masks + (slot * n + i) * S.mask_words + (b >> 6), 1ull << (b & 63));
                     const int64_t len = N.rowptr[i + 1] - N.rowptr[i];
                     nch = (int)((len + CHUNK - 1) / CHUNK);
                     if (PLASTIC) push_plastic_row(N, S, t, b, i);
@@ -396,11 +406,23 @@ __device__ __forceinline__ void push_range(const DevNet& N, const DevState& S, i
 // Step engine, kernel 2: the spikes of step t+1-n_delay (they arrive at step t+1) are scattered
 // into the accumulator that step t+1 reads; each block takes a contiguous share of every list.
 // ---------------------------------------------------------------------------------------------
+// The spike-mask slot that step t+1 records into starts empty (it last held step t-n_delay, whose
+// propagation ran at step t-1).
+__device__ __forceinline__ void clear_mask_slot(const DevNet& N, const DevState& S, int64_t t)
+{
+    if (!S.masks) return;
+    const int64_t words = N.n * S.mask_words;
+    unsigned long long* m = S.masks + pos_mod(t + 1, N.R) * words;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < words; k += (int64_t)gridDim.x * blockDim.x)
+        m[k] = 0ull;
+}
+
 template <typename AccT, int LANES>
 __global__ void __launch_bounds__(256) k_push(const DevNet N, const DevState S, int64_t t)
 {
     __shared__ int32_t pre[MAX_SEG];
     __shared__ int32_t s_total;
+    clear_mask_slot(N, S, t);
     if (t + 1 - N.n_delay < 0) return;
     AccT* acc = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
     const int64_t slot = pos_mod(t + 1 - N.n_delay, N.R);
@@ -415,6 +437,45 @@ __global__ void __launch_bounds__(256) k_push(const DevNet N, const DevState S, 
         push_range<AccT, LANES>(N, S, t, q, acc, pre, g0, g1, threadIdx.x / LANES, blockDim.x / LANES,
                                 threadIdx.x % LANES, S.reset_tick, S.stop_tick, 0);
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pull propagation (step engine, kernel 2 alternative): every postsynaptic neuron j gathers its
+// incoming entries whose presynaptic neuron spiked at step s = t+1-n_delay, for the instances of
+// one 64-bit mask word per thread. The sums are exact integers, so push and pull give identical
+// accumulators; pull reads the whole connectome once per step for all instances, push only the
+// rows of the spikes (it pays off only when a large share of neurons fires every step).
+// ---------------------------------------------------------------------------------------------
+template <typename AccT> __device__ __forceinline__ AccT pull_weight(const DevNet& N, int64_t e);
+template <> __device__ __forceinline__ int32_t pull_weight<int32_t>(const DevNet& N, int64_t e) { return N.ccnt[e]; }
+template <> __device__ __forceinline__ int64_t pull_weight<int64_t>(const DevNet& N, int64_t e) { return N.cwfx[e]; }
+
+template <typename AccT>
+__global__ void __launch_bounds__(256) k_pull(const DevNet N, const DevState S, int64_t t)
+{
+    clear_mask_slot(N, S, t);
+    const int64_t s = t + 1 - N.n_delay;
+    if (s < 0) return;
+    AccT* acc = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
+    const int W = S.mask_words;
+    const unsigned long long* M = S.masks + pos_mod(s, N.R) * N.n * W;
+    const int64_t total = N.n * W;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = p / W;
+        const int w = (int)(p - j * W);
+        const int64_t e1 = N.colptr[j + 1];
+        for (int64_t e = N.colptr[j]; e < e1; e++) {
+            unsigned long long m = __ldg(M + (int64_t)N.cpre[e] * W + w);
+            if (!m) continue;
+            const AccT c = pull_weight<AccT>(N, e);
+            while (m) {
+                const int32_t b = w * 64 + __ffsll((long long)m) - 1;
+                m &= m - 1;
+                if (s < S.reset_tick[b] || t + 1 >= S.stop_tick[b]) continue;
+                acc[(int64_t)b * N.n_pad + j] += c;     // (b, j) belongs to this thread alone
+            }
+        }
     }
 }
 

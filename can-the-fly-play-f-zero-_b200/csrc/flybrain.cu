@@ -136,6 +136,15 @@ struct fb_brain {
     int32_t* pl_post = nullptr;
     int32_t* ppost_neuron = nullptr;  // neuron of each compact plastic target
     int32_t* ppost_of = nullptr;
+    // pull propagation (built on first use): connectome by postsynaptic neuron + spike masks
+    int64_t* colptr = nullptr;
+    int32_t* cpre = nullptr;
+    int16_t* ccnt = nullptr;
+    int64_t* cwfx = nullptr;
+    unsigned long long* masks = nullptr;
+    int32_t mask_words = 0;
+    int64_t mask_from = 0;        // first spike step whose mask is recorded (pull reads only these)
+    bool masks_dirty = false;     // steps ran without recording masks (the persistent engine)
     float* pw = nullptr;
     float* w0 = nullptr;
     // state
@@ -191,6 +200,7 @@ struct fb_brain {
         N.rowptr = rowptr; N.col = col; N.cnt = cnt; N.wfx = wfx;
         N.n_pl = n_pl; N.n_ppost = n_ppost; N.pl_rowptr = pl_rowptr; N.pl_pidx = pl_pidx; N.pl_q0 = pl_q0;
         N.ppost_of = ppost_of;
+        N.colptr = colptr; N.cpre = cpre; N.ccnt = ccnt; N.cwfx = cwfx;
         N.L32 = L32; N.L64 = L64;
         return N;
     }
@@ -202,6 +212,7 @@ struct fb_brain {
         S.items = items; S.item_count = item_count; S.cap_c = cap_c; S.group = list_group;
         S.n_groups = n_groups; S.n_seg = n_seg; S.seg_pairs = seg_pairs; S.reset_tick = reset_tick;
         S.stop_tick = stop_tick; S.err = err_d; S.seed = seed;
+        S.masks = masks; S.mask_words = mask_words;
         return S;
     }
 };
@@ -214,7 +225,7 @@ int free_all(fb_brain* h)
                     h->pl_pre, h->pl_post, h->ppost_neuron,
                     h->v, h->g, h->ref, h->ext_idx, h->p_ext, h->bias_ext, h->acc[0], h->acc[1], h->pring,
                     h->items, h->item_count, h->reset_tick, h->stop_tick, h->fly_mask, h->bar, h->abort_flag,
-                    h->ext_tab, h->ext_off};
+                    h->ext_tab, h->ext_off, h->colptr, h->cpre, h->ccnt, h->cwfx, h->masks};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (void* p : h->graveyard) cudaFree(p);
@@ -298,6 +309,28 @@ int build_ext_table(fb_brain* h)
 
 int dispatch_step(fb_brain* h, const StepArgs& A, bool raster, bool record, cudaStream_t st);
 int dispatch_push(fb_brain* h, int64_t t, cudaStream_t st);
+int dispatch_pull(fb_brain* h, int64_t t, cudaStream_t st);
+
+// Build what pull propagation needs: the connectome by postsynaptic neuron and the spike-mask
+// ring (zeroed; masks are recorded from the current step on). The device must be idle.
+int enable_pull(fb_brain* h)
+{
+    if (h->masks) return FB_OK;
+    HostCsc Cc;
+    build_csc(h->hc, Cc);
+    int rc;
+    if ((rc = upload(&h->colptr, Cc.colptr, &h->bytes))) return rc;
+    if ((rc = upload(&h->cpre, Cc.pre, &h->bytes))) return rc;
+    if (h->acc_mode == 0) { if ((rc = upload(&h->ccnt, Cc.cnt, &h->bytes))) return rc; }
+    else if ((rc = upload(&h->cwfx, Cc.wfx, &h->bytes))) return rc;
+    h->mask_words = (h->B + 63) / 64;
+    const size_t words = (size_t)h->R * h->n * h->mask_words;
+    if ((rc = dalloc(&h->masks, words, &h->bytes))) return rc;
+    CU(cudaMemset(h->masks, 0, words * sizeof(unsigned long long)));
+    h->mask_from = h->t;
+    h->masks_dirty = false;
+    return FB_OK;
+}
 
 }  // namespace
 
@@ -519,6 +552,11 @@ extern "C" int fb_reset(fb_brain* h, const int32_t* flies, int32_t n_flies, void
     h->launches += 1;
     if (all) {
         h->t = 0;
+        if (h->masks) {
+            CU(cudaMemsetAsync(h->masks, 0, (size_t)h->R * h->n * h->mask_words * sizeof(unsigned long long), st));
+            h->mask_from = 0;
+            h->masks_dirty = false;
+        }
         CU(cudaMemsetAsync(h->item_count, 0, (size_t)h->R * h->n_groups * h->n_seg * sizeof(int32_t), st));
     }
     k_set_ticks<<<(h->B + 255) / 256, 256, 0, st>>>(h->reset_tick, mask, h->B, h->t);
@@ -580,7 +618,16 @@ extern "C" int fb_set_schedule(fb_brain* h, int32_t engine, int32_t propagation,
     if (lanes != 0 && lanes != 8 && lanes != 16 && lanes != 32) return fail(FB_ERR_ARG, "lanes must be 8, 16 or 32");
     if (engine == FB_ENGINE_PERSISTENT && h->plan.group == 0)
         return fail(FB_ERR_UNSUPPORTED, "the persistent engine cannot hold one instance of %lld neurons on chip", (long long)h->n);
-    if (propagation == FB_PROP_PULL) return fail(FB_ERR_UNSUPPORTED, "pull propagation is not built in this version");
+    const int new_prop = propagation >= 0 ? propagation : h->prop;
+    const int new_engine = (engine != 0 || h->engine != 0) ? engine : h->engine;
+    if (new_prop == FB_PROP_PULL && new_engine == FB_ENGINE_PERSISTENT)
+        return fail(FB_ERR_UNSUPPORTED, "pull propagation runs on the step engine only");
+    if (new_prop == FB_PROP_PULL && !h->masks) {
+        CU(cudaSetDevice(h->device));
+        CU(cudaDeviceSynchronize());
+        int rc = enable_pull(h);
+        if (rc) return rc;
+    }
     if (engine != 0 || h->engine != 0) h->engine = engine;
     if (propagation >= 0) h->prop = propagation;
     if (lanes) h->lanes = lanes;
@@ -652,6 +699,19 @@ template <typename AccT> void launch_push(fb_brain* h, int64_t t, int blocks, cu
     else k_push<AccT, 32><<<blocks, 256, 0, st>>>(N, S, t);
 }
 
+int dispatch_pull(fb_brain* h, int64_t t, cudaStream_t st)
+{
+    const int64_t work = h->n * h->mask_words;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)h->sm_count * 16));
+    const DevNet N = h->net();
+    const DevState S = h->state();
+    if (h->acc_mode == 0) k_pull<int32_t><<<blocks, 256, 0, st>>>(N, S, t);
+    else k_pull<int64_t><<<blocks, 256, 0, st>>>(N, S, t);
+    CU(cudaGetLastError());
+    h->launches += 1;
+    return FB_OK;
+}
+
 int dispatch_push(fb_brain* h, int64_t t, cudaStream_t st)
 {
     const int blocks = (int)std::min<int64_t>(std::max<int64_t>(h->sm_count, (int64_t)h->B * 16), (int64_t)h->sm_count * 8);
@@ -679,8 +739,10 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
     const bool record = step_counts || step_digest;
     const int32_t words = (int32_t)((h->n_ext + 31) / 32);
     int engine = h->engine;
-    if (engine == FB_ENGINE_AUTO) engine = (h->plan.group > 0 && !h->f64) ? FB_ENGINE_PERSISTENT : FB_ENGINE_STEP;
+    if (engine == FB_ENGINE_AUTO)
+        engine = (h->plan.group > 0 && !h->f64 && h->prop == FB_PROP_PUSH) ? FB_ENGINE_PERSISTENT : FB_ENGINE_STEP;
     if (engine == FB_ENGINE_PERSISTENT && h->plan.group > 0 && !h->f64) {
+        h->masks_dirty = h->masks != nullptr;     // no spike masks recorded for these steps
         PersistArgs P{};
         P.t0 = h->t; P.step0 = h->step_no; P.steps = steps; P.kicks = kicks; P.words = words;
         P.counts = counts_out; P.step_counts = step_counts; P.step_digest = step_digest;
@@ -692,13 +754,20 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         if (rc) return fail(FB_ERR_CUDA, "persistent launch: %s", cudaGetErrorString((cudaError_t)rc));
         h->launches += h->plan.launches_per_run;
     } else {
+        if (h->masks && h->masks_dirty) {          // masks restart empty from this step on
+            CU(cudaMemsetAsync(h->masks, 0, (size_t)h->R * h->n * h->mask_words * sizeof(unsigned long long), st));
+            h->mask_from = h->t;
+            h->masks_dirty = false;
+        }
         for (int32_t s = 0; s < steps; s++) {
             StepArgs A{};
             A.t = h->t + s; A.step_no = h->step_no + (uint32_t)s; A.s = s; A.kicks = kicks; A.words = words;
             A.counts = counts_out; A.step_counts = step_counts; A.step_digest = step_digest;
             int rc = dispatch_step(h, A, kicks != nullptr, record, st);
             if (rc) return rc;
-            rc = dispatch_push(h, A.t, st);
+            // pull only for spike steps whose masks were recorded (else the work items serve)
+            const bool pull = h->prop == FB_PROP_PULL && h->masks && A.t + 1 - h->n_delay >= h->mask_from;
+            rc = pull ? dispatch_pull(h, A.t, st) : dispatch_push(h, A.t, st);
             if (rc) return rc;
         }
     }

@@ -126,6 +126,36 @@ inline std::string prepare_csr(const int64_t* indptr, const int32_t* indices, co
     return "";
 }
 
+// The connectome by postsynaptic neuron (the pull propagation's gather order): for post j the
+// entries colptr[j]..colptr[j+1]-1 hold (presynaptic neuron, count or Q32.32 weight), by pre.
+struct HostCsc {
+    std::vector<int64_t> colptr;      // (n+1)
+    std::vector<int32_t> pre;         // (nnz)
+    std::vector<int16_t> cnt;         // (nnz) acc_mode 0
+    std::vector<int64_t> wfx;         // (nnz) acc_mode 1
+};
+
+inline void build_csc(const HostCsr& H, HostCsc& C)
+{
+    const int64_t n = H.n, nnz = H.nnz;
+    C = HostCsc{};
+    C.colptr.assign(n + 1, 0);
+    for (int64_t k = 0; k < nnz; k++) C.colptr[H.ix[k] + 1] += 1;
+    for (int64_t j = 0; j < n; j++) C.colptr[j + 1] += C.colptr[j];
+    std::vector<int64_t> fill(C.colptr.begin(), C.colptr.end() - 1);
+    C.pre.resize(nnz);
+    if (H.acc_mode == 0) C.cnt.resize(nnz);
+    else C.wfx.resize(nnz);
+    for (int64_t i = 0; i < n; i++)
+        for (int64_t k = H.ip[i]; k < H.ip[i + 1]; k++) {
+            const int64_t q = fill[H.ix[k]]++;
+            const int64_t src = H.rp[i] + (k - H.ip[i]);
+            C.pre[q] = (int32_t)i;
+            if (H.acc_mode == 0) C.cnt[q] = H.pcnt[src];
+            else C.wfx[q] = H.pwfx[src];
+        }
+}
+
 struct PlasticPlan {
     int64_t n_pl = 0;
     int32_t n_ppost = 0;

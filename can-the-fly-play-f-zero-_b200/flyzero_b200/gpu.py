@@ -219,7 +219,8 @@ class BatchBrain:
         self._wrap()
 
     def set_schedule(self, engine: str | None = None, propagation: str | None = None, lanes: int = 0):
-        """engine: 'auto' | 'step' | 'persistent'; propagation: 'push' | 'pull'; lanes: 8/16/32."""
+        """engine: 'auto' | 'step' | 'persistent'; propagation: 'push' | 'pull' (pull runs on the step
+        engine; its first n_delay steps after the switch still push); lanes: 8/16/32 per work item."""
         e = {None: 0, "auto": 0, "step": 1, "persistent": 2}[engine]
         pr = {None: -1, "push": 0, "pull": 1}[propagation]
         _lib.check(self._L.fb_set_schedule(self._h, e, pr, int(lanes)))
@@ -232,3 +233,56 @@ class BatchBrain:
         s = np.asarray(steps_per_instance, np.int64)
         stop = np.where(s < 0, np.iinfo(np.int64).max, self.t + s)
         self.stop_tick.copy_(torch.as_tensor(stop, device=self.device))
+
+    # ---- schedule autotuner -------------------------------------------------------------------
+    def schedule_candidates(self):
+        """Schedules worth timing for this engine: (engine, propagation, lanes)."""
+        info = self.info()
+        cands = []
+        if info.group > 0 and not info.f64:
+            cands += [("persistent", "push", lanes) for lanes in (8, 16, 32)]
+        cands += [("step", "push", 8), ("step", "push", 32), ("step", "pull", 8)]
+        return cands
+
+    def autotune(self, steps: int = 166, candidates=None, apply: bool = True) -> dict:
+        """Time each candidate schedule on the next ``steps`` steps of the simulation and keep the
+        fastest. Every schedule computes bit-identical results, so the simulation simply continues
+        through the trials: the call advances every instance by (len(candidates)) * (steps + warm-up)
+        steps, best done right after a reset. Also reports the measured activity and the modelled
+        bytes of push (16 + 14 * out-degree per spike) and pull (14 per connectome entry + masks)."""
+        import torch
+
+        cands = list(candidates) if candidates is not None else self.schedule_candidates()
+        st = torch.cuda.current_stream(self.device)
+        warm = self.info().n_delay + 2          # pull needs n_delay recorded steps before it gathers
+        rowlen = torch.as_tensor(np.diff(self.indptr), device=self.device)
+        times, spikes, edges = {}, 0, 0
+        counts = torch.empty((self.B, self.n), dtype=torch.int32, device=self.device)
+        for c in cands:
+            self.set_schedule(c[0], c[1], c[2])
+            self.run_steps(warm, counts=counts)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            self.run_steps(steps, counts=counts)
+            b.record(st)
+            b.synchronize()
+            times[c] = a.elapsed_time(b) / steps
+            per_neuron = counts.sum(0).to(torch.int64)
+            spikes += int(per_neuron.sum())
+            edges += int((per_neuron * rowlen).sum())
+        self.check()
+        best = choose_schedule(times)
+        if apply:
+            self.set_schedule(*best)
+        trials = len(cands) * steps
+        return {"best": best, "ms_per_step": {"/".join(map(str, k)): v for k, v in times.items()},
+                "spikes_per_step": spikes / max(trials, 1),
+                "push_bytes_per_step": (16 * spikes + 14 * edges) / max(trials, 1),
+                "pull_bytes_per_step": 14.0 * len(self.indices) + 8.0 * self.n * ((self.B + 63) // 64)}
+
+
+def choose_schedule(ms_per_step: dict):
+    """The fastest schedule of a {schedule: ms per step} table (the first listed on ties)."""
+    if not ms_per_step:
+        raise ValueError("no schedule was timed")
+    return min(ms_per_step, key=lambda k: (ms_per_step[k], list(ms_per_step).index(k)))

@@ -103,6 +103,25 @@ int main()
             CHECK(segment_capacity(H, n_pad, group, seg_pairs, n_seg) == want);
         }
 
+        // the by-postsynaptic copy holds every entry once, in pre order within each column
+        {
+            HostCsc Cc;
+            build_csc(H, Cc);
+            CHECK((int64_t)Cc.colptr.size() == n + 1 && Cc.colptr[n] == nnz);
+            std::vector<int64_t> seen(n, 0);
+            for (int64_t j = 0; j < n; j++)
+                for (int64_t q = Cc.colptr[j]; q < Cc.colptr[j + 1]; q++) {
+                    const int32_t i = Cc.pre[q];
+                    if (q > Cc.colptr[j]) CHECK(Cc.pre[q - 1] < i);
+                    int64_t k = H.ip[i];
+                    while (k < H.ip[i + 1] && H.ix[k] != j) k++;
+                    CHECK(k < H.ip[i + 1]);
+                    const int64_t src = H.rp[i] + (k - H.ip[i]);
+                    if (integral) CHECK(Cc.cnt[q] == H.pcnt[src]);
+                    else CHECK(Cc.wfx[q] == H.pwfx[src]);
+                    seen[j]++;
+                }
+        }
         // plastic plans: a random subset, then a superset; weights and ring survive the re-plan
         if (nnz == 0) continue;
         std::vector<int64_t> pos1, pos2;

@@ -370,3 +370,75 @@ def test_persistent_short_delays_bias_and_plastic(torch, dt):
         total += c.sum()
     _compare_state(torch, gb, eo)
     assert total > 0
+
+
+@pytest.mark.parametrize("B,float_weights", [(3, False), (70, False), (3, True)])
+def test_pull_propagation_is_exact(torch, B, float_weights):
+    """Pull (gather by postsynaptic neuron over spike masks, 64 instances per mask word) gives the
+    same accumulators as push: bit-exact vs the oracle across a push -> pull switch, a partial reset
+    and per-instance run lengths; integer counts (INT32) and float weights (Q32.32)."""
+    from flyzero_b200.brain import LIFParams
+
+    conn = cx.synthetic(4096, seed=9)
+    w = conn.weights.copy()
+    if float_weights:
+        w.data = w.data * np.float32(0.75)
+    idx, rate = wl.high_activity_inputs(conn.n, seed=9)
+    gb = _bb(w, LIFParams(), B, "step", seed=3)
+    gb.set_input(idx, rate)
+    eo = O.EngineOracle(w, O.Params(), batch=B, seed=3)
+    j = eo.slots(idx)
+    eo.p_ext[:, j] = rate * np.float32(0.1 / 1000.0)
+    np.testing.assert_array_equal(gb.run_steps(30).cpu().numpy(), eo.run_steps(30))     # push
+    gb.set_schedule("step", "pull")
+    assert gb.info().propagation == 1
+    np.testing.assert_array_equal(gb.run_steps(60).cpu().numpy(), eo.run_steps(60))     # pull after n_delay
+    flies = [1] if B < 64 else [1, 65]
+    gb.reset(flies)
+    eo.reset_flies(flies)
+    lengths = np.full(B, -1)
+    lengths[0] = 25
+    gb.set_run_length(lengths)
+    stop = np.full(B, 2 ** 62, np.int64)
+    stop[0] = eo.t + 25
+    np.testing.assert_array_equal(gb.run_steps(50).cpu().numpy(), eo.run_steps(50, stop_tick=stop))
+    _compare_state(torch, gb, eo)
+
+
+def test_persistent_then_pull_then_persistent(torch):
+    """Switching engines mid-run: spike masks restart after persistent steps (push serves the gap)."""
+    from flyzero_b200.brain import LIFParams
+
+    conn = cx.synthetic(4096, seed=12)
+    idx, rate = wl.high_activity_inputs(conn.n, seed=12)
+    gb = _bb(conn.weights, LIFParams(), 2, "persistent", seed=8)
+    gb.set_input(idx, rate)
+    eo = O.EngineOracle(conn.weights, O.Params(), batch=2, seed=8)
+    j = eo.slots(idx)
+    eo.p_ext[:, j] = rate * np.float32(0.1 / 1000.0)
+    for engine, prop, steps in (("persistent", "push", 40), ("step", "pull", 45), ("persistent", "push", 30),
+                                ("step", "pull", 10), ("step", "pull", 35)):
+        gb.set_schedule(engine, prop)
+        np.testing.assert_array_equal(gb.run_steps(steps).cpu().numpy(), eo.run_steps(steps))
+    _compare_state(torch, gb, eo)
+
+
+def test_autotune_keeps_results_exact(torch):
+    """The autotuner times every schedule on the running simulation and keeps the fastest; the
+    simulation it advanced is still bit-exact."""
+    from flyzero_b200.brain import LIFParams
+
+    conn = cx.synthetic(8192, seed=4)
+    idx, rate = wl.config1_inputs(conn.n, seed=4)
+    gb = _bb(conn.weights, LIFParams(), 4, "auto", seed=2)
+    gb.set_input(idx, rate * 3)
+    eo = O.EngineOracle(conn.weights, O.Params(), batch=4, seed=2)
+    j = eo.slots(idx)
+    eo.p_ext[:, j] = (rate * 3) * np.float32(0.1 / 1000.0)
+    rep = gb.autotune(steps=20)
+    assert rep["best"] in gb.schedule_candidates()
+    assert len(rep["ms_per_step"]) == len(gb.schedule_candidates())
+    advanced = gb.t
+    eo.run_steps(advanced)
+    np.testing.assert_array_equal(gb.run_steps(50).cpu().numpy(), eo.run_steps(50))
+    _compare_state(torch, gb, eo)
