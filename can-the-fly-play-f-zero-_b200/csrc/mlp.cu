@@ -1,0 +1,281 @@
+// Kernels of the learned surrogate (include/flysurrogate.h): a BF16 tensor-core GEMM with fused
+// epilogues (bias, GELU, GELU gradient, transposed copies for the backward pass), the Poisson
+// negative log-likelihood, column sums (bias gradients), Adam, and FP32 -> BF16 conversion.
+//
+// Every GEMM of the MLP's training step is written as C = A * B^T with both operands stored
+// K-contiguous (the forward pass keeps transposed copies of activations and weights for the
+// backward pass), so one kernel serves them all: 128 x 64 output tiles, 8 warps of 32 x 32,
+// BF16 m16n8k16 tensor-core MMAs with FP32 accumulation, operands staged in padded shared
+// memory (conflict-free 32-bit fragment loads).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include <cstdint>
+
+#include "../../include/flybrain.h"
+#include "../../include/flysurrogate.h"
+
+namespace fb {
+void set_last_error(const char* msg);
+}
+
+namespace {
+
+constexpr int BM = 128, BN = 64, BK = 32, PADK = BK + 8;
+
+__device__ __forceinline__ uint16_t f2bf(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_grad(float z)
+{
+    return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * expf(-0.5f * z * z) * 0.39894228040143268f;
+}
+
+// 8 consecutive bf16 of row `row` from column k (zero outside [0, rows) x [0, K))
+__device__ __forceinline__ void load8(const uint16_t* X, int row, int k, int rows, int K, int ld, uint16_t* dst)
+{
+    if (row < rows && k + 8 <= K) {
+        *reinterpret_cast<uint4*>(dst) = __ldg(reinterpret_cast<const uint4*>(X + (int64_t)row * ld + k));
+    } else {
+#pragma unroll
+        for (int u = 0; u < 8; u++) dst[u] = (row < rows && k + u < K) ? X[(int64_t)row * ld + k + u] : (uint16_t)0;
+    }
+}
+
+__device__ __forceinline__ uint32_t lds32(const uint16_t* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+struct Epi {
+    int32_t mode, ldo, ldo_t;
+    const float* bias;
+    const float* zin;
+    float* out_f32;
+    uint16_t* out_bf16;
+    uint16_t* out_bf16_t;
+};
+
+__device__ __forceinline__ void epilogue(const Epi& e, int M, int N, int i, int j, float v)
+{
+    if (i >= M || j >= N) return;
+    const int64_t o = (int64_t)i * e.ldo + j;
+    switch (e.mode) {
+    case FS_EPI_F32: e.out_f32[o] = v; break;
+    case FS_EPI_BIAS_F32: e.out_f32[o] = v + e.bias[j]; break;
+    case FS_EPI_BIAS_GELU: {
+        const float z = v + e.bias[j];
+        e.out_f32[o] = z;
+        const uint16_t h = f2bf(gelu(z));
+        e.out_bf16[o] = h;
+        if (e.out_bf16_t) e.out_bf16_t[(int64_t)j * e.ldo_t + i] = h;
+        break;
+    }
+    default: {   // FS_EPI_GELU_GRAD
+        const uint16_t d = f2bf(v * gelu_grad(e.zin[o]));
+        e.out_bf16[o] = d;
+        if (e.out_bf16_t) e.out_bf16_t[(int64_t)j * e.ldo_t + i] = d;
+    }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gemm(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B, int M,
+                                              int N, int K, int lda, int ldb, Epi e)
+{
+    __shared__ __align__(16) uint16_t As[BM][PADK];
+    __shared__ __align__(16) uint16_t Bs[BN][PADK];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const int wm = warp & 3, wn = warp >> 2;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += BK) {
+        for (int c = tid; c < BM * 4; c += 256) load8(A, m0 + (c >> 2), k0 + (c & 3) * 8, M, K, lda, &As[c >> 2][(c & 3) * 8]);
+        for (int c = tid; c < BN * 4; c += 256) load8(B, n0 + (c >> 2), k0 + (c & 3) * 8, N, K, ldb, &Bs[c >> 2][(c & 3) * 8]);
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 16) {
+            uint32_t a[2][4], b[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const int r = wm * 32 + i * 16 + g;
+                a[i][0] = lds32(&As[r][kk + 2 * t4]);
+                a[i][1] = lds32(&As[r + 8][kk + 2 * t4]);
+                a[i][2] = lds32(&As[r][kk + 2 * t4 + 8]);
+                a[i][3] = lds32(&As[r + 8][kk + 2 * t4 + 8]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int c = wn * 32 + j * 8 + g;
+                b[j][0] = lds32(&Bs[c][kk + 2 * t4]);
+                b[j][1] = lds32(&Bs[c][kk + 2 * t4 + 8]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], a[i], b[j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int r = m0 + wm * 32 + i * 16 + g, c = n0 + wn * 32 + j * 8 + 2 * t4;
+            epilogue(e, M, N, r, c, acc[i][j][0]);
+            epilogue(e, M, N, r, c + 1, acc[i][j][1]);
+            epilogue(e, M, N, r + 8, c, acc[i][j][2]);
+            epilogue(e, M, N, r + 8, c + 1, acc[i][j][3]);
+        }
+}
+
+__global__ void k_poisson(const float* z, const float* y, int M, int D, double* loss, uint16_t* dz, int ldd, uint16_t* dz_t)
+{
+    __shared__ double part[8];
+    double s = 0.0;
+    const int64_t total = (int64_t)M * D;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < total; p += (int64_t)gridDim.x * blockDim.x) {
+        const float zz = z[p], yy = y[p];
+        const float ez = expf(zz);
+        s += (double)ez - (double)yy * (double)zz;
+        const uint16_t d = f2bf((ez - yy) / (float)M);
+        const int64_t m = p / D, k = p - m * D;
+        dz[m * ldd + k] = d;
+        if (dz_t) dz_t[k * M + m] = d;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += part[w];
+        atomicAdd(loss, t);
+    }
+}
+
+__global__ void k_colsum(const uint16_t* X, int M, int N, int ld, float* grad)
+{
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    float s = 0.0f;
+    for (int i = 0; i < M; i++) s += __bfloat162float(__ushort_as_bfloat16(X[(int64_t)i * ld + j]));
+    grad[j] = s;
+}
+
+__global__ void k_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
+                       float c1, float c2, uint16_t* wb, uint16_t* wbt, int rows, int cols, int ldt)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const float gg = g[p];
+        const float mm = b1 * m[p] + (1.0f - b1) * gg;
+        const float vv = b2 * v[p] + (1.0f - b2) * gg * gg;
+        m[p] = mm;
+        v[p] = vv;
+        const float ww = w[p] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+        w[p] = ww;
+        const uint16_t h = f2bf(ww);
+        if (wb) wb[p] = h;
+        if (wbt) {
+            const int64_t r = p / cols, c = p - r * cols;
+            wbt[c * ldt + r] = h;
+        }
+    }
+}
+
+__global__ void k_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* out_t, int rows, int cols, int ldt)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const uint16_t h = f2bf(x[p]);
+        if (out) out[p] = h;
+        if (out_t) {
+            const int64_t r = p / cols, c = p - r * cols;
+            out_t[c * ldt + r] = h;
+        }
+    }
+}
+
+int fail(const char* msg)
+{
+    fb::set_last_error(msg);
+    return FB_ERR_ARG;
+}
+
+int cuda_status()
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) return FB_OK;
+    fb::set_last_error(cudaGetErrorString(e));
+    return FB_ERR_CUDA;
+}
+
+unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
+
+}  // namespace
+
+extern "C" int fs_gemm(const uint16_t* A, const uint16_t* B, int32_t M, int32_t N, int32_t K, int32_t lda, int32_t ldb,
+                       int32_t epi, const float* bias, const float* zin, float* out_f32, uint16_t* out_bf16,
+                       uint16_t* out_bf16_t, int32_t ldo, int32_t ldo_t, void* stream)
+{
+    if (!A || !B || M <= 0 || N <= 0 || K <= 0) return fail("fs_gemm: bad operands");
+    if (lda % 8 || ldb % 8 || lda < K || ldb < K) return fail("fs_gemm: lda, ldb must be multiples of 8 and >= K");
+    if (epi < FS_EPI_F32 || epi > FS_EPI_GELU_GRAD) return fail("fs_gemm: unknown epilogue");
+    if ((epi == FS_EPI_F32 || epi == FS_EPI_BIAS_F32 || epi == FS_EPI_BIAS_GELU) && !out_f32)
+        return fail("fs_gemm: out_f32 needed");
+    if ((epi == FS_EPI_BIAS_F32 || epi == FS_EPI_BIAS_GELU) && !bias) return fail("fs_gemm: bias needed");
+    if ((epi == FS_EPI_BIAS_GELU || epi == FS_EPI_GELU_GRAD) && !out_bf16) return fail("fs_gemm: out_bf16 needed");
+    if (epi == FS_EPI_GELU_GRAD && !zin) return fail("fs_gemm: zin needed");
+    Epi e{epi, ldo, ldo_t, bias, zin, out_f32, out_bf16, out_bf16_t};
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    k_gemm<<<grid, 256, 0, (cudaStream_t)stream>>>(A, B, M, N, K, lda, ldb, e);
+    return cuda_status();
+}
+
+extern "C" int fs_poisson_nll(const float* z, const float* y, int32_t M, int32_t D, double* loss_sum, uint16_t* dz,
+                              int32_t ldd, uint16_t* dz_t, void* stream)
+{
+    if (!z || !y || !loss_sum || !dz || M <= 0 || D <= 0 || ldd < D) return fail("fs_poisson_nll: bad arguments");
+    k_poisson<<<blocks_for((int64_t)M * D), 256, 0, (cudaStream_t)stream>>>(z, y, M, D, loss_sum, dz, ldd, dz_t);
+    return cuda_status();
+}
+
+extern "C" int fs_colsum(const uint16_t* X, int32_t M, int32_t N, int32_t ld, float* grad, void* stream)
+{
+    if (!X || !grad || M <= 0 || N <= 0 || ld < N) return fail("fs_colsum: bad arguments");
+    k_colsum<<<(N + 127) / 128, 128, 0, (cudaStream_t)stream>>>(X, M, N, ld, grad);
+    return cuda_status();
+}
+
+extern "C" int fs_adam(float* w, const float* grad, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                       float eps, int32_t t, uint16_t* w_bf16, uint16_t* w_bf16_t, int32_t rows, int32_t cols,
+                       int32_t ldt, void* stream)
+{
+    if (!w || !grad || !m || !v || n <= 0 || t < 1) return fail("fs_adam: bad arguments");
+    if (w_bf16_t && ((int64_t)rows * cols != n || ldt < rows))
+        return fail("fs_adam: the transposed copy needs rows * cols == n and ldt >= rows");
+    const float c1 = 1.0f - powf(beta1, (float)t), c2 = 1.0f - powf(beta2, (float)t);
+    k_adam<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(w, grad, m, v, n, lr, beta1, beta2, eps, c1, c2, w_bf16,
+                                                            w_bf16_t, rows, cols, ldt);
+    return cuda_status();
+}
+
+extern "C" int fs_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* out_t, int32_t rows, int32_t cols,
+                          int32_t ldt, void* stream)
+{
+    if (!x || n <= 0 || (!out && !out_t)) return fail("fs_to_bf16: bad arguments");
+    if (out_t && ((int64_t)rows * cols != n || ldt < rows))
+        return fail("fs_to_bf16: the transposed copy needs rows * cols == n and ldt >= rows");
+    k_to_bf16<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(x, n, out, out_t, rows, cols, ldt);
+    return cuda_status();
+}

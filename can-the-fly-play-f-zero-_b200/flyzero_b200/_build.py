@@ -16,7 +16,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(ROOT, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libflybrain.so")
-SOURCES = ["flybrain.cu", "static_run.cu"]
+SOURCES = ["flybrain.cu", "static_run.cu", "mlp.cu"]
 HEADERS = ["common.cuh", "engine.cuh", "persist.cuh", "host_prep.hpp", "plastic.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -37,7 +37,7 @@ def _stale(out: str, deps: list) -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(OUT_DIR, exist_ok=True)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "..", "include", "flybrain.h")]
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "..", "include", h) for h in ("flybrain.h", "flysurrogate.h")]
     deps += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))]
     if not force and not _stale(LIB, deps):
         return LIB

@@ -65,6 +65,14 @@ SIGNATURES = {
                                  C.c_int32, vp]),
     "fb_run_static": (C.c_int, [C.POINTER(Params), C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp, vp, C.c_uint32,
                                 C.c_uint32, C.c_int64, C.c_int32, C.c_int32, vp, vp]),
+    # include/flysurrogate.h
+    "fs_gemm": (C.c_int, [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp,
+                          vp, C.c_int32, C.c_int32, vp]),
+    "fs_poisson_nll": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32, vp, vp]),
+    "fs_colsum": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp]),
+    "fs_adam": (C.c_int, [vp, vp, vp, vp, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32, vp, vp,
+                          C.c_int32, C.c_int32, C.c_int32, vp]),
+    "fs_to_bf16": (C.c_int, [vp, C.c_int64, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp]),
 }
 
 

@@ -1,4 +1,4 @@
-"""The C-ABI library builds, loads without a GPU and exports every function include/flybrain.h
+"""The C-ABI library builds, loads without a GPU and exports every function include/*.h
 declares (no compute calls: this runs on CPU)."""
 
 import ctypes as C
@@ -8,9 +8,12 @@ import re
 from conftest import ROOT
 
 
-def _declared(header="flybrain.h"):
-    text = open(os.path.join(ROOT, "include", header)).read()
-    return sorted(set(re.findall(r"^\s*int\s+(fb_\w+)\s*\(", text, flags=re.M)))
+def _declared(headers=("flybrain.h", "flysurrogate.h")):
+    names = set()
+    for h in headers:
+        text = open(os.path.join(ROOT, "include", h)).read()
+        names |= set(re.findall(r"^\s*int\s+((?:fb|fs)_\w+)\s*\(", text, flags=re.M))
+    return sorted(names)
 
 
 def test_header_declares_the_boundary():

@@ -1,0 +1,100 @@
+"""The surrogate's CUDA kernels: the BF16 tensor-core GEMM and its epilogues against a plain
+PyTorch FP32 reference, the training step's gradients against the CPU FP64 oracle, and training."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import mlp_oracle as MO
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _p(t):
+    return None if t is None else C.c_void_p(t.data_ptr())
+
+
+@pytest.mark.parametrize("M,N,K", [(300, 70, 200), (128, 64, 32), (37, 10, 16), (4096, 512, 1280)])
+def test_gemm_and_epilogues_match_torch_fp32(torch, M, N, K):
+    from flyzero_b200 import _lib
+
+    L = _lib.load()
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    A = torch.randn((M, K), device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn((N, K), device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.randn(N, device="cuda", generator=g)
+    ref = A.float() @ B.float().T                               # FP32 reference of the same bf16 operands
+    tol = dict(rtol=2e-5 * K, atol=2e-5 * K)
+    out = torch.empty((M, N), device="cuda")
+    _lib.check(L.fs_gemm(_p(A), _p(B), M, N, K, K, K, 0, None, None, _p(out), None, None, N, 0, None))
+    torch.testing.assert_close(out, ref, **tol)
+    # bias + GELU: pre-activation, bf16 activation and its transpose
+    z = torch.empty((M, N), device="cuda")
+    h = torch.empty((M, N), dtype=torch.bfloat16, device="cuda")
+    ht = torch.empty((N, M), dtype=torch.bfloat16, device="cuda")
+    _lib.check(L.fs_gemm(_p(A), _p(B), M, N, K, K, K, 1, _p(bias), None, _p(z), _p(h), _p(ht), N, M, None))
+    torch.testing.assert_close(z, ref + bias, **tol)
+    want = torch.nn.functional.gelu(z).to(torch.bfloat16)
+    torch.testing.assert_close(h.float(), want.float(), rtol=1e-2, atol=1e-2)
+    assert torch.equal(ht.T, h)
+    # GELU gradient epilogue: d = C * gelu'(zin)
+    zin = torch.randn((M, N), device="cuda", generator=g)
+    d = torch.empty((M, N), dtype=torch.bfloat16, device="cuda")
+    _lib.check(L.fs_gemm(_p(A), _p(B), M, N, K, K, K, 3, None, _p(zin), None, _p(d), None, N, 0, None))
+    zz = zin.clone().requires_grad_(True)
+    torch.nn.functional.gelu(zz).backward(ref)
+    torch.testing.assert_close(d.float(), zz.grad, rtol=1e-2, atol=1e-2 * float(ref.abs().max()))
+
+
+def test_training_gradients_match_fp64_oracle(torch):
+    from flyzero_b200.surrogate import MLP
+
+    net = MLP(seed=1)
+    rng = np.random.default_rng(2)
+    M = 256
+    X = rng.normal(0, 1, (M, 1280)).astype(np.float32)
+    Y = rng.poisson(2.0, (M, 10)).astype(np.float32)
+    Xd, Yd = torch.as_tensor(X, device="cuda"), torch.as_tensor(Y, device="cuda")
+    net.forward(Xd, training=True)
+    loss = float(net.backward(Yd))
+    params = net.params_f64()
+    L, grads = MO.loss_and_grads(params, MO.bf16_round(X), Y.astype(np.float64))
+    assert abs(loss - L) <= 2e-3 * abs(L)
+    for li, ((gW, gb), (oW, ob)) in enumerate(zip(net.grads, grads)):
+        for got, want in ((gW.cpu().numpy(), oW), (gb.cpu().numpy(), ob)):
+            rel = np.linalg.norm(got - want) / np.linalg.norm(want)
+            cos = float(np.sum(got * want) / (np.linalg.norm(got) * np.linalg.norm(want)))
+            assert rel < 3e-2 and cos > 0.9995, (li, rel, cos)
+
+
+def test_training_learns_a_poisson_teacher(torch):
+    from flyzero_b200.surrogate import MLP
+
+    rng = np.random.default_rng(3)
+    Wt = rng.normal(0, 0.02, (10, 1280)).astype(np.float32)
+    def batch(M):
+        X = rng.normal(0, 1, (M, 1280)).astype(np.float32)
+        Y = rng.poisson(np.exp(X @ Wt.T + 0.5)).astype(np.float32)
+        return torch.as_tensor(X, device="cuda"), torch.as_tensor(Y, device="cuda")
+    net = MLP(seed=4, lr=1e-3)
+    Xv, Yv = batch(4096)
+    net.forward(Xv, training=True)
+    first = float(net.backward(Yv))
+    for _ in range(150):
+        net.train_step(*batch(1024))
+    net.forward(Xv, training=True)
+    last = float(net.backward(Yv))
+    # the teacher's own NLL is the floor; training closes most of the gap from the start
+    z = Xv.cpu().numpy() @ Wt.T + 0.5
+    floor = float(np.mean(np.sum(np.exp(z) - Yv.cpu().numpy() * z, 1)))
+    assert last < first and (last - floor) < 0.5 * (first - floor), (first, last, floor)
