@@ -9,17 +9,19 @@
 //               weight pw enters as the Q32.32 delta q32(pw) - q32(w0), pushed at spike time.
 //   state       v[B][n], g[B][n] (f32 or f64), ref[B][n] i8
 //   inputs      ext_idx[n] i32, p_ext[B][n_ext] f32, bias_ext[B][n_ext] f32
-//   delay line  acc[2][B][n_pad] (i32 or i64): synaptic input of the next two steps, rows padded
-//               to 16 entries so that every row starts on a 64-byte boundary (TMA bulk copies);
+//   delay line  acc[S][B][n_pad] (i32 or i64): synaptic input of the next S ticks (slot = tick mod
+//               S, S = 2 x the persistent engine's epoch, at least 2), rows padded to 16 entries so
+//               that every row starts on a 64-byte boundary (TMA bulk copies);
 //               items[R][n_groups][n_seg][cap_c] int2: spike work lists of the last R = n_delay+1
 //               steps, one per instance group and segment (the pairs one persistent CTA owns);
-//               item_count[R][n_groups][n_seg]; pring[R][B][n_ppost] i64: plastic input;
+//               item_count[R][n_groups][n_seg]; pring[R_pl][B][n_ppost] i64: plastic input (R_pl = n_delay + epoch: a slot
+//               is cleared by its reader at least one epoch before anyone pushes into it again);
 //               with pull propagation also masks[R][n][ceil(B/64)] u64: which instances each
 //               neuron spiked in, and the connectome by postsynaptic neuron (colptr, cpre, ccnt/cwfx)
 //
 // The delay line is "deferred push": the fixed-weight rows of the spikes of step s are scattered
-// into acc only at step s + n_delay - 1, right before they arrive, so only two accumulator slots
-// (instead of n_delay) are live. Fixed weights never change during a run and integer addition is
+// into acc only shortly before they arrive (the step engine at step s + n_delay - 1, the
+// persistent engine one epoch ahead), so only S accumulator slots (instead of n_delay) are live. Fixed weights never change during a run and integer addition is
 // order-free, so this equals the reference's push-at-spike-time ring (brain.py:54-56) exactly.
 // Plastic weights may change between runs, so their rows are pushed at spike time.
 #pragma once
@@ -30,6 +32,7 @@ namespace fb {
 struct DevNet {
     int64_t n, n_pad;
     int32_t B, n_delay, R, n_ref;
+    int32_t R_pl;              // plastic input ring slots: n_delay + the persistent engine's epoch
     const int64_t* rowptr;
     const int32_t* col;
     const int16_t* cnt;
@@ -57,8 +60,8 @@ struct DevState {
     int32_t n_ext;
     const float* p_ext;
     const float* bias_ext;
-    void* acc0;
-    void* acc1;
+    void* acc;                 // [n_slots][B][n_pad]
+    int32_t n_slots;
     int64_t* pring;
     int2* items;               // [R][n_groups][n_seg][cap_c]
     int32_t* item_count;       // [R][n_groups][n_seg]
@@ -92,6 +95,12 @@ __device__ __forceinline__ bool bits_differ(float a, float b) { return __float_a
 __device__ __forceinline__ bool bits_differ(double a, double b)
 {
     return __double_as_longlong(a) != __double_as_longlong(b);
+}
+
+// accumulator slot of tick t
+template <typename AccT> __device__ __forceinline__ AccT* acc_slot(const DevNet& N, const DevState& S, int64_t t)
+{
+    return reinterpret_cast<AccT*>(S.acc) + pos_mod(t, S.n_slots) * (int64_t)N.B * N.n_pad;
 }
 
 template <typename Real> __device__ __forceinline__ const Lif<Real>& lif_of(const DevNet& N);
@@ -180,7 +189,7 @@ __device__ __forceinline__ void push_plastic_row(const DevNet& N, const DevState
     const int64_t p0 = N.pl_rowptr[i], p1 = N.pl_rowptr[i + 1];
     if (p0 == p1) return;
     unsigned long long* dst = reinterpret_cast<unsigned long long*>(
-        S.pring + (pos_mod(t + N.n_delay, N.R) * N.B + b) * (int64_t)N.n_ppost);
+        S.pring + (pos_mod(t + N.n_delay, N.R_pl) * N.B + b) * (int64_t)N.n_ppost);
     const float* w = S.pw + (int64_t)b * N.n_pl;
     for (int64_t k = p0; k < p1; k++) {
         const int64_t d = to_q32(w[k]) - N.pl_q0[k];
@@ -193,7 +202,7 @@ template <typename Real>
 __device__ __forceinline__ Real take_plastic(const DevNet& N, const DevState& S, int64_t t, int32_t b, int32_t i)
 {
     const int32_t pp = N.ppost_of[i];
-    int64_t* q = S.pring + (pos_mod(t, N.R) * N.B + b) * (int64_t)N.n_ppost + pp;
+    int64_t* q = S.pring + (pos_mod(t, N.R_pl) * N.B + b) * (int64_t)N.n_ppost + pp;
     const int64_t px = __ldcg(reinterpret_cast<const long long*>(q));
     if (px != 0) *q = 0;
     return from_q32<Real>(px);
@@ -225,7 +234,7 @@ __global__ void __launch_bounds__(256) k_update(const DevNet N, const DevState S
     if (blockIdx.x == 0)       // the lists consumed by the push at t-1 start empty again
         for (int32_t k = threadIdx.x; k < S.n_groups * S.n_seg; k += blockDim.x)
             S.item_count[pos_mod(t - N.n_delay, N.R) * S.n_groups * S.n_seg + k] = 0;
-    AccT* acc = reinterpret_cast<AccT*>((t & 1) ? S.acc1 : S.acc0);
+    AccT* acc = acc_slot<AccT>(N, S, t);
     Real* V = reinterpret_cast<Real*>(S.v);
     Real* G = reinterpret_cast<Real*>(S.g);
     const int64_t slot = pos_mod(t, N.R);
@@ -417,14 +426,16 @@ __device__ __forceinline__ void clear_mask_slot(const DevNet& N, const DevState&
         m[k] = 0ull;
 }
 
+// `do_push` 0: the arrivals of t+1 were pushed ahead already (by the persistent engine); only the
+// mask slot is cleared.
 template <typename AccT, int LANES>
-__global__ void __launch_bounds__(256) k_push(const DevNet N, const DevState S, int64_t t)
+__global__ void __launch_bounds__(256) k_push(const DevNet N, const DevState S, int64_t t, int do_push)
 {
     __shared__ int32_t pre[MAX_SEG];
     __shared__ int32_t s_total;
     clear_mask_slot(N, S, t);
-    if (t + 1 - N.n_delay < 0) return;
-    AccT* acc = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
+    if (!do_push || t + 1 - N.n_delay < 0) return;
+    AccT* acc = acc_slot<AccT>(N, S, t + 1);
     const int64_t slot = pos_mod(t + 1 - N.n_delay, N.R);
     for (int32_t q = 0; q < S.n_groups; q++) {
         if (threadIdx.x < 32) {
@@ -457,7 +468,7 @@ __global__ void __launch_bounds__(256) k_pull(const DevNet N, const DevState S, 
     clear_mask_slot(N, S, t);
     const int64_t s = t + 1 - N.n_delay;
     if (s < 0) return;
-    AccT* acc = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
+    AccT* acc = acc_slot<AccT>(N, S, t + 1);
     const int W = S.mask_words;
     const unsigned long long* M = S.masks + pos_mod(s, N.R) * N.n * W;
     const int64_t total = N.n * W;

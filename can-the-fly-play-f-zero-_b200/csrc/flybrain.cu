@@ -72,7 +72,7 @@ __global__ void k_consts(double dt, double tau_m, double tau_syn, double f_poiss
 }
 
 template <typename Real>
-__global__ void k_reset(Real* v, Real* g, int8_t* ref, void* acc0, void* acc1, int acc_bytes, int64_t* pring,
+__global__ void k_reset(Real* v, Real* g, int8_t* ref, void* acc, int32_t n_slots, int acc_bytes, int64_t* pring,
                         int32_t R, int32_t B, int64_t n, int64_t n_pad, int32_t n_ppost, const uint8_t* fly_mask,
                         Real v_rest)
 {
@@ -85,12 +85,10 @@ __global__ void k_reset(Real* v, Real* g, int8_t* ref, void* acc0, void* acc1, i
         g[p] = (Real)0;
         ref[p] = 0;
         const int64_t a = (int64_t)b * n_pad + (p - (int64_t)b * n);
-        if (acc_bytes == 4) {
-            ((int32_t*)acc0)[a] = 0;
-            ((int32_t*)acc1)[a] = 0;
-        } else {
-            ((int64_t*)acc0)[a] = 0;
-            ((int64_t*)acc1)[a] = 0;
+        for (int32_t k = 0; k < n_slots; k++) {
+            const int64_t o = (int64_t)k * B * n_pad + a;
+            if (acc_bytes == 4) ((int32_t*)acc)[o] = 0;
+            else ((int64_t*)acc)[o] = 0;
         }
     }
     const int64_t ptotal = (int64_t)R * B * n_ppost;
@@ -113,7 +111,7 @@ struct fb_brain {
     int device = 0;
     fb_params params{};
     int64_t n = 0, n_pad = 0, nnz = 0, nnz_pad = 0;
-    int32_t B = 0, n_delay = 1, n_ref = 0, R = 2;
+    int32_t B = 0, n_delay = 1, n_ref = 0, R = 2, R_pl = 2;
     int acc_mode = 0;      // 0 INT32 counts, 1 Q32.32
     int f64 = 0;
     uint32_t seed = 0;
@@ -161,7 +159,10 @@ struct fb_brain {
     HostCsr hc;                       // host copy of the CSR for re-planning the plastic entries
     PlasticPlan plastic;              // current plastic plan
     // delay line
-    void* acc[2] = {nullptr, nullptr};
+    void* acc = nullptr;          // [n_slots][B][n_pad]
+    int32_t n_slots = 2;
+    int32_t epoch = 1;            // persistent engine: steps per grid barrier
+    int64_t pushed_until = 1;     // the arrivals of every tick < pushed_until are in acc
     int64_t* pring = nullptr;
     int2* items = nullptr;
     int32_t* item_count = nullptr;
@@ -196,7 +197,7 @@ struct fb_brain {
     DevNet net() const
     {
         DevNet N{};
-        N.n = n; N.n_pad = n_pad; N.B = B; N.n_delay = n_delay; N.R = R; N.n_ref = n_ref;
+        N.n = n; N.n_pad = n_pad; N.B = B; N.n_delay = n_delay; N.R = R; N.R_pl = R_pl; N.n_ref = n_ref;
         N.rowptr = rowptr; N.col = col; N.cnt = cnt; N.wfx = wfx;
         N.n_pl = n_pl; N.n_ppost = n_ppost; N.pl_rowptr = pl_rowptr; N.pl_pidx = pl_pidx; N.pl_q0 = pl_q0;
         N.ppost_of = ppost_of;
@@ -208,7 +209,7 @@ struct fb_brain {
     {
         DevState S{};
         S.v = v; S.g = g; S.ref = ref; S.pw = pw; S.ext_idx = ext_idx; S.n_ext = (int32_t)n_ext;
-        S.p_ext = p_ext; S.bias_ext = bias_ext; S.acc0 = acc[0]; S.acc1 = acc[1]; S.pring = pring;
+        S.p_ext = p_ext; S.bias_ext = bias_ext; S.acc = acc; S.n_slots = n_slots; S.pring = pring;
         S.items = items; S.item_count = item_count; S.cap_c = cap_c; S.group = list_group;
         S.n_groups = n_groups; S.n_seg = n_seg; S.seg_pairs = seg_pairs; S.reset_tick = reset_tick;
         S.stop_tick = stop_tick; S.err = err_d; S.seed = seed;
@@ -223,7 +224,7 @@ int free_all(fb_brain* h)
 {
     void* ptrs[] = {h->rowptr, h->col, h->cnt, h->wfx, h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->pw, h->w0,
                     h->pl_pre, h->pl_post, h->ppost_neuron,
-                    h->v, h->g, h->ref, h->ext_idx, h->p_ext, h->bias_ext, h->acc[0], h->acc[1], h->pring,
+                    h->v, h->g, h->ref, h->ext_idx, h->p_ext, h->bias_ext, h->acc, h->pring,
                     h->items, h->item_count, h->reset_tick, h->stop_tick, h->fly_mask, h->bar, h->abort_flag,
                     h->ext_tab, h->ext_off, h->colptr, h->cpre, h->ccnt, h->cwfx, h->masks};
     for (void* p : ptrs)
@@ -249,10 +250,10 @@ int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
     std::vector<float> pwh = remap_weights(h->plastic, old_pw, P, B);
     std::vector<int64_t> old_ring;
     if (h->pring && h->n_ppost > 0) {
-        old_ring.resize((size_t)h->R * B * h->n_ppost);
+        old_ring.resize((size_t)h->R_pl * B * h->n_ppost);
         CU(cudaMemcpy(old_ring.data(), h->pring, old_ring.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
     }
-    std::vector<int64_t> ring = remap_ring(h->plastic, old_ring, P, (int64_t)h->R * B);
+    std::vector<int64_t> ring = remap_ring(h->plastic, old_ring, P, (int64_t)h->R_pl * B);
     void* olds[] = {h->pl_rowptr, h->pl_pidx, h->pl_q0, h->ppost_of, h->w0, h->pring, h->pl_pre, h->pl_post,
                     h->ppost_neuron};
     for (void* p : olds)
@@ -401,14 +402,17 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
     TRY(dalloc(&h->bias_ext, 1, tb));
     const size_t ab = h->acc_mode == 0 ? 4 : 8;
     const size_t nbp = (size_t)batch * h->n_pad;
-    TRY(dalloc((char**)&h->acc[0], nbp * ab, tb));
-    TRY(dalloc((char**)&h->acc[1], nbp * ab, tb));
-    CU(cudaMemset(h->acc[0], 0, nbp * ab));
-    CU(cudaMemset(h->acc[1], 0, nbp * ab));
     TRY(dalloc(&h->bar, 1, tb));
     TRY(dalloc(&h->abort_flag, 1, tb));
     int dev_sms2 = h->sm_count;
     h->plan = plan_persistent(h->n, h->n_pad, h->B, h->f64 != 0, h->n_ref, h->n_delay, (int)ab, dev_sms2, h->device);
+    // the persistent engine runs epochs of K steps between grid barriers: the spikes of an epoch
+    // arrive two epochs later at the earliest when 2K + 1 <= n_delay; 2K accumulator slots
+    h->epoch = h->plan.group > 0 ? std::max(1, std::min(MAX_EPOCH, (h->n_delay - 1) / 2)) : 1;
+    h->n_slots = 2 * h->epoch;
+    h->R_pl = h->n_delay + h->epoch;
+    TRY(dalloc((char**)&h->acc, nbp * ab * h->n_slots, tb));
+    CU(cudaMemset(h->acc, 0, nbp * ab * h->n_slots));
     h->list_group = h->plan.group > 0 ? h->plan.group : h->B;
     h->n_groups = (h->B + h->list_group - 1) / h->list_group;
     TRY(install_plastic(h, pos));
@@ -470,7 +474,7 @@ extern "C" int fb_get_info(const fb_brain* h, fb_info* o)
     o->acc_mode = h->acc_mode; o->f64 = h->f64; o->engine = h->engine; o->propagation = h->prop;
     o->lanes = h->lanes; o->group = h->plan.group; o->ctas = h->plan.ctas; o->n_plastic = h->n_pl;
     o->n_ext = h->n_ext; o->t = h->t; o->step_no = h->step_no; o->launches = h->launches;
-    o->item_capacity = h->cap_c; o->bytes_device = (int64_t)h->bytes;
+    o->item_capacity = h->cap_c; o->bytes_device = (int64_t)h->bytes; o->epoch = h->epoch;
     o->decay_syn = h->consts64[0]; o->decay_m = h->consts64[1]; o->kick = h->consts64[2];
     return FB_OK;
 }
@@ -543,15 +547,16 @@ extern "C" int fb_reset(fb_brain* h, const int32_t* flies, int32_t n_flies, void
     const int blocks = (int)std::min<int64_t>((total + 255) / 256, (int64_t)h->sm_count * 16);
     const int ab = h->acc_mode == 0 ? 4 : 8;
     if (h->f64)
-        k_reset<double><<<blocks, 256, 0, st>>>((double*)h->v, (double*)h->g, h->ref, h->acc[0], h->acc[1], ab, h->pring,
-                                                h->R, h->B, h->n, h->n_pad, h->n_ppost, mask, h->params.v_rest);
+        k_reset<double><<<blocks, 256, 0, st>>>((double*)h->v, (double*)h->g, h->ref, h->acc, h->n_slots, ab, h->pring,
+                                                h->R_pl, h->B, h->n, h->n_pad, h->n_ppost, mask, h->params.v_rest);
     else
-        k_reset<float><<<blocks, 256, 0, st>>>((float*)h->v, (float*)h->g, h->ref, h->acc[0], h->acc[1], ab, h->pring,
-                                               h->R, h->B, h->n, h->n_pad, h->n_ppost, mask, (float)h->params.v_rest);
+        k_reset<float><<<blocks, 256, 0, st>>>((float*)h->v, (float*)h->g, h->ref, h->acc, h->n_slots, ab, h->pring,
+                                               h->R_pl, h->B, h->n, h->n_pad, h->n_ppost, mask, (float)h->params.v_rest);
     CU(cudaGetLastError());
     h->launches += 1;
     if (all) {
         h->t = 0;
+        h->pushed_until = 1;          // tick 0 receives nothing; nothing later is pushed
         if (h->masks) {
             CU(cudaMemsetAsync(h->masks, 0, (size_t)h->R * h->n * h->mask_words * sizeof(unsigned long long), st));
             h->mask_from = 0;
@@ -690,13 +695,13 @@ int dispatch_step(fb_brain* h, const StepArgs& A, bool raster, bool record, cuda
     return FB_OK;
 }
 
-template <typename AccT> void launch_push(fb_brain* h, int64_t t, int blocks, cudaStream_t st)
+template <typename AccT> void launch_push(fb_brain* h, int64_t t, int do_push, int blocks, cudaStream_t st)
 {
     const DevNet N = h->net();
     const DevState S = h->state();
-    if (h->lanes == 8) k_push<AccT, 8><<<blocks, 256, 0, st>>>(N, S, t);
-    else if (h->lanes == 16) k_push<AccT, 16><<<blocks, 256, 0, st>>>(N, S, t);
-    else k_push<AccT, 32><<<blocks, 256, 0, st>>>(N, S, t);
+    if (h->lanes == 8) k_push<AccT, 8><<<blocks, 256, 0, st>>>(N, S, t, do_push);
+    else if (h->lanes == 16) k_push<AccT, 16><<<blocks, 256, 0, st>>>(N, S, t, do_push);
+    else k_push<AccT, 32><<<blocks, 256, 0, st>>>(N, S, t, do_push);
 }
 
 int dispatch_pull(fb_brain* h, int64_t t, cudaStream_t st)
@@ -715,8 +720,9 @@ int dispatch_pull(fb_brain* h, int64_t t, cudaStream_t st)
 int dispatch_push(fb_brain* h, int64_t t, cudaStream_t st)
 {
     const int blocks = (int)std::min<int64_t>(std::max<int64_t>(h->sm_count, (int64_t)h->B * 16), (int64_t)h->sm_count * 8);
-    if (h->acc_mode == 0) launch_push<int32_t>(h, t, blocks, st);
-    else launch_push<int64_t>(h, t, blocks, st);
+    const int do_push = t + 1 >= h->pushed_until;      // else pushed ahead by the persistent engine
+    if (h->acc_mode == 0) launch_push<int32_t>(h, t, do_push, blocks, st);
+    else launch_push<int64_t>(h, t, do_push, blocks, st);
     CU(cudaGetLastError());
     h->launches += 1;
     return FB_OK;
@@ -748,11 +754,14 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         P.counts = counts_out; P.step_counts = step_counts; P.step_digest = step_digest;
         P.bar = h->bar; P.abort_flag = h->abort_flag; P.ext_tab = h->ext_tab; P.ext_off = h->ext_off;
         P.trace = ((int64_t)steps * h->plan.ctas * TRACE_SLOTS <= h->trace_cap) ? h->trace : nullptr;
+        P.pushed_until = h->pushed_until;
+        P.epoch = h->epoch;
         CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
         int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
                                    record, h->lanes, st);
         if (rc) return fail(FB_ERR_CUDA, "persistent launch: %s", cudaGetErrorString((cudaError_t)rc));
         h->launches += h->plan.launches_per_run;
+        h->pushed_until = std::max<int64_t>(h->pushed_until, h->t + steps + 1);
     } else {
         if (h->masks && h->masks_dirty) {          // masks restart empty from this step on
             CU(cudaMemsetAsync(h->masks, 0, (size_t)h->R * h->n * h->mask_words * sizeof(unsigned long long), st));
@@ -766,9 +775,11 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
             int rc = dispatch_step(h, A, kicks != nullptr, record, st);
             if (rc) return rc;
             // pull only for spike steps whose masks were recorded (else the work items serve)
-            const bool pull = h->prop == FB_PROP_PULL && h->masks && A.t + 1 - h->n_delay >= h->mask_from;
+            const bool pull = h->prop == FB_PROP_PULL && h->masks && A.t + 1 - h->n_delay >= h->mask_from &&
+                              A.t + 1 >= h->pushed_until;
             rc = pull ? dispatch_pull(h, A.t, st) : dispatch_push(h, A.t, st);
             if (rc) return rc;
+            h->pushed_until = std::max<int64_t>(h->pushed_until, A.t + 2);
         }
     }
     h->t += steps;

@@ -8,17 +8,22 @@
 // it by bulk stores from a zero page), the CSR rows of the spikes that arrive next step, and the
 // reductions they scatter.
 //
-// Warp roles of a CTA (all steps, separated by one grid barrier per step):
-//   neuron warps (U, 26): stage the slice, advance every owned pair, then draw the next step's
+// Epochs: the spikes of a step arrive n_delay steps later, so with K = (n_delay - 1) / 2 (at most
+// MAX_EPOCH) the spikes of one epoch of K steps cannot arrive before the epoch after next. One grid
+// barrier per epoch suffices: during an epoch the push warps scatter the work items that arrive in
+// the next epoch into their accumulator slots (2K slots: tick mod 2K), while the neuron and
+// listing warps step through the epoch with only a CTA-level barrier between steps.
+//
+// Warp roles of a CTA:
+//   neuron warps (U, 26): per step, stage the slice (the next step's load is issued before the
+//     kicks when it lies in the same epoch), advance every owned pair, draw the next step's
 //     Poisson kicks into a shared bitmap;
-//   push warps (4): scatter the work items that arrive next step into the other accumulator;
-//   listing warps (2): list the previous step's spikes (counts, plastic rows, work items of this
-//     CTA's segment of the group's list).
-// A spike of step s is listed during step s+1 and first scattered during step s+n_delay-1, so
-// the engine needs n_delay >= 3. Three bitmaps rotate: map[s%3] holds the kicks of step s, then
-// (overwritten by the neuron warps) its spikes; map[(s+1)%3] receives the next kicks; the listing
-// warps read and clear map[(s-1)%3]. Every wait is bounded: after ~4 s a CTA raises the timeout
-// flag and every CTA returns.
+//   listing warps (2): per step, list the previous step's spikes (counts, plastic rows, work items
+//     of this CTA's segment of the group's list);
+//   push warps (4): per epoch, scatter this CTA's share of the items arriving in the next epoch.
+// Three bitmaps rotate: map[s%3] holds the kicks of step s, then (overwritten by the neuron warps)
+// its spikes; map[(s+1)%3] receives the next kicks; the listing warps read and clear map[(s-1)%3].
+// Every wait is bounded: after ~4 s a CTA raises the timeout flag and every CTA returns.
 #pragma once
 #include "engine.cuh"
 
@@ -28,7 +33,9 @@ constexpr int PT = 1024;                // threads per CTA
 constexpr int ZERO_PAGE = 4096;         // shared-memory zeros, the source of the clearing bulk stores
 constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulator slice
 constexpr int SPK_BUF = 1024;           // spikes of one CTA and step listed in parallel
+constexpr int IT_BUF = 384;             // work items of one CTA's epoch push staged in shared memory
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
+constexpr int MAX_EPOCH = 8;            // steps per epoch at most (accumulator slots: twice that)
 
 constexpr int PUSH_WARPS = 4;                              // warps that scatter arriving items ...
 constexpr int LIST_WARPS = 2;                              // ... that list the previous step's spikes ...
@@ -59,12 +66,14 @@ struct PersistArgs {
     const int2* ext_tab;      // per CTA: input pairs {k | instance << 18, ext slot}
     const int32_t* ext_off;   // (ctas + 1) offsets into ext_tab
     long long* trace;         // nullptr, or (steps, ctas, TRACE_SLOTS) clock64 stamps of each step's phases
+    int64_t pushed_until;     // the arrivals of every tick < pushed_until are in the accumulators
+    int32_t epoch;            // K: steps between grid barriers (2K accumulator slots, 2K + 1 <= n_delay)
 };
 
-// Phase stamps (per step and CTA; SM clock cycles, compare within a CTA): 0 step start, 1 neuron
-// warps start, 2 slice in shared memory, 3 neurons advanced, 4 next kicks drawn, 5 barrier
-// arrival of the neuron warps, 6 barrier exit, 7 push warps start, 8 listing warps done,
-// 9 push warps' segment prefix ready, 10 push warps done.
+// Phase stamps (per step and CTA; SM clock cycles, compare within a CTA): 0 step start, 1 slice
+// requested, 2 slice in shared memory, 3 neurons advanced, 4 next kicks drawn, 8 listing warps
+// done with the previous step; per epoch, at its first step: 7 push warps start, 10 push warps
+// done; at its last step: 5 grid-barrier arrival, 6 grid-barrier exit (9 unused).
 constexpr int TRACE_SLOTS = 11;
 
 // ---- PTX helpers: mbarrier, TMA 1-D bulk copy, proxy fences, acquire load --------------------
@@ -158,7 +167,7 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
 
 // Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
 struct PersistSmem {
-    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, total, words_per_map;
+    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, total, words_per_map;
     __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
     {
         words_per_map = (per + 4 * PT) / 32 + 1;
@@ -169,12 +178,13 @@ struct PersistSmem {
         g = v + per * 4;
         kbits = g + per * 4;                 // three bitmaps: the kicks of a step become its spikes
         ref = kbits + 3 * words_per_map * 4;
-        misc = (ref + per + 15) / 16 * 16;   // 64 active flags, 8 counters
-        scan = misc + 64 + 32;               // 32 block-scan partial sums
-        pre = scan + 128;                    // 2 x MAX_SEG segment prefix entries (step parity)
-        spk = pre + 8 * MAX_SEG;             // SPK_BUF spikes being listed
+        misc = (ref + per + 15) / 16 * 16;   // 64 active flags, 16 counters
+        scan = misc + 64 + 64;               // 32 block-scan partial sums
+        pre = scan + 128;                    // MAX_EPOCH x MAX_SEG segment prefix entries
+        spk = pre + 4 * MAX_EPOCH * MAX_SEG; // SPK_BUF spikes being listed
         ticks = spk + 4 * SPK_BUF;           // reset and stop ticks of up to 64 instances
-        total = ticks + 2 * 64 * 8;
+        items = ticks + 2 * 64 * 8;          // IT_BUF staged work items of an epoch's push
+        total = items + 16 * IT_BUF;
     }
 };
 
@@ -194,6 +204,8 @@ __device__ __forceinline__ bool u_sync_or(bool pred)
     return out != 0;
 }
 __device__ __forceinline__ void push_sync() { asm volatile("bar.sync 2, %0;" ::"n"(PUSH_THREADS) : "memory"); }
+// step boundary between the neuron warps and the listing warps (the push warps run free in an epoch)
+__device__ __forceinline__ void ul_sync() { asm volatile("bar.sync 4, %0;" ::"n"(U_THREADS + LIST_THREADS) : "memory"); }
 __device__ __forceinline__ void list_sync() { asm volatile("bar.sync 3, %0;" ::"n"(LIST_THREADS) : "memory"); }
 
 // bulk store shared -> global (16-byte aligned, size a multiple of 16), tracked by bulk groups
@@ -373,6 +385,156 @@ __device__ __forceinline__ void list_spikes(const DevNet& N, const DevState& S, 
     }
 }
 
+// Bulk load of this CTA's accumulator slice (`bytes` from global `src`) into shared memory,
+// completing on `mbar` (one transaction per step: the waits alternate parity).
+template <typename AccT>
+__device__ __forceinline__ void issue_slice(const AccT* src, AccT* sacc, uint32_t bytes, uint64_t* mbar)
+{
+    fence_proxy_async_global();
+    mbar_expect_tx(mbar, bytes);
+    for (uint32_t off = 0; off < bytes; off += LOAD_PIECE)
+        tma_load_1d(reinterpret_cast<uint8_t*>(sacc) + off, reinterpret_cast<const uint8_t*>(src) + off,
+                    min((uint32_t)LOAD_PIECE, bytes - off), mbar);
+}
+
+// Push warps: scatter this CTA's share of the work items that arrive at ticks [a0, a1) into their
+// accumulator slots, one arrival tick after the other (its list is the spikes of tick a - n_delay).
+template <typename AccT, int LANES>
+__device__ __forceinline__ void push_arrivals(const DevNet& N, const DevState& S, int32_t q, int32_t b0, int64_t a0,
+                                              int64_t a1, int32_t* s_pre, int32_t* s_cnt, const int64_t* s_reset,
+                                              const int64_t* s_stop, int ptid)
+{
+    for (int64_t a = a0; a < a1; a++) {
+        const int64_t sp = a - N.n_delay;
+        if (sp < 0) continue;
+        const int par = (int)(a & 1);
+        int32_t* pre = s_pre + par * MAX_SEG;
+        if (ptid < 32) {
+            const int32_t tot = segment_prefix(S, pos_mod(sp, N.R), q, pre);
+            if (ptid == 0) s_cnt[2 + par] = tot;
+        }
+        push_sync();
+        const int64_t total = s_cnt[2 + par];   // this CTA's share: a contiguous range of items
+        const int64_t g0 = total * blockIdx.x / gridDim.x, g1 = total * (blockIdx.x + 1) / gridDim.x;
+        push_range<AccT, LANES>(N, S, a - 1, q, acc_slot<AccT>(N, S, a), pre, g0, g1, ptid / LANES,
+                                PUSH_THREADS / LANES, ptid % LANES, s_reset, s_stop, b0);
+    }
+}
+
+// Push warps, one epoch: this CTA's shares of the lists arriving at ticks [a0, a1) (at most
+// MAX_EPOCH lists) scattered with every memory access of a phase in flight at once:
+//   1. the segment prefixes of all lists (each warp takes whole lists);
+//   2. every item of the shares loaded once (thread j takes a contiguous run), filtered by the
+//      instance ticks, recorded in shared memory as {first entry, entries, instance, arrival}, and
+//      numbered by 8-entry groups (a scan over the push threads);
+//   3. the groups spread over all push threads, two in flight per thread.
+// Items beyond IT_BUF follow list by list (push_range).
+template <typename AccT, int LANES>
+__device__ __forceinline__ void push_epoch(const DevNet& N, const DevState& S, int32_t q, int32_t b0, int64_t a0,
+                                           int64_t a1, int32_t* s_pre, int32_t* s_cnt, int32_t* scratch, int4* recs,
+                                           const int64_t* s_reset, const int64_t* s_stop, int ptid)
+{
+    const int nl = (int)(a1 - a0);
+    const int warp = ptid >> 5;
+    for (int k = warp; k < nl; k += PUSH_WARPS) {
+        const int64_t sp = a0 + k - N.n_delay;
+        int32_t tot = 0;
+        if (sp >= 0) tot = segment_prefix(S, pos_mod(sp, N.R), q, s_pre + k * MAX_SEG);
+        if ((ptid & 31) == 0) s_cnt[8 + k] = sp >= 0 ? tot : 0;       // list totals: s_cnt[8 .. 8+MAX_EPOCH)
+    }
+    push_sync();
+    // shares and their flattened offsets (every thread computes the same small table)
+    int64_t g0[MAX_EPOCH], off[MAX_EPOCH + 1];
+    off[0] = 0;
+#pragma unroll
+    for (int k = 0; k < MAX_EPOCH; k++) {
+        const int64_t total = k < nl ? s_cnt[8 + k] : 0;
+        g0[k] = total * blockIdx.x / gridDim.x;
+        off[k + 1] = off[k] + (total * (blockIdx.x + 1) / gridDim.x - g0[k]);
+    }
+    const int64_t M = off[MAX_EPOCH];
+    const int32_t m = (int32_t)min(M, (int64_t)IT_BUF);
+    // 2. stage the items: thread ptid takes records [ptid * c, (ptid + 1) * c)
+    const int32_t c = (m + PUSH_THREADS - 1) / PUSH_THREADS;
+    const int32_t r0 = min(ptid * c, m), r1 = min(r0 + c, m);
+    int groups = 0;
+    for (int32_t j = r0; j < r1; j++) {
+        int k = 0;
+        while (k + 1 < MAX_EPOCH && off[k + 1] <= j) k++;
+        const int64_t g = g0[k] + (j - off[k]);
+        const int32_t* pre = s_pre + k * MAX_SEG;
+        int32_t lo = 0, hi = S.n_seg - 1;                        // first segment whose prefix exceeds g
+        while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if (pre[mid] > g) hi = mid;
+            else lo = mid + 1;
+        }
+        const int64_t sp = a0 + k - N.n_delay;
+        const int2 item = __ldcg(list_of(S, pos_mod(sp, N.R), q, lo) + (g - (lo > 0 ? pre[lo - 1] : 0)));
+        const int32_t bl = (item.y >> CHUNK_BITS) - b0;
+        int32_t len = item.y & ((1 << CHUNK_BITS) - 1);
+        if (sp < s_reset[bl] || a0 + k >= s_stop[bl]) len = 0;
+        recs[j] = make_int4(item.x, len, bl | (k << 8), 0);
+        groups += (len + 7) / 8;
+    }
+    int all = 0;
+    int base = block_scan(groups, &all, scratch, ptid, PUSH_THREADS, []() { push_sync(); });
+    for (int32_t j = r0; j < r1; j++) {
+        recs[j].w = base;
+        base += (recs[j].y + 7) / 8;
+    }
+    push_sync();
+    // 3. the 8-entry groups, two in flight per thread
+    const int64_t np = N.n_pad;
+    const int64_t slot_stride = (int64_t)N.B * np;
+    AccT* acc0 = reinterpret_cast<AccT*>(S.acc);
+    auto locate = [&](int32_t gi) {                              // last record whose first group <= gi
+        int32_t lo = 0, hi = m - 1;
+        while (lo < hi) {
+            const int32_t mid = (lo + hi + 1) >> 1;
+            if (recs[mid].w <= gi) lo = mid;
+            else hi = mid - 1;
+        }
+        return recs[lo];
+    };
+    auto target = [&](const int4& r) {
+        const int k = r.z >> 8, bl = r.z & 0xff;
+        return acc0 + pos_mod(a0 + k, S.n_slots) * slot_stride + (int64_t)(b0 + bl) * np;
+    };
+    for (int32_t ga = ptid; ga < all; ga += 2 * PUSH_THREADS) {
+        const int32_t gb = ga + PUSH_THREADS;
+        const int4 ra = locate(ga);
+        Edges8<AccT> ea, eb;
+        ea.load(N, (int64_t)(uint32_t)ra.x + 8 * (int64_t)(ga - ra.w));
+        int4 rb = ra;
+        if (gb < all) {
+            rb = locate(gb);
+            eb.load(N, (int64_t)(uint32_t)rb.x + 8 * (int64_t)(gb - rb.w));
+        }
+        AccT* ta = target(ra);
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+            if (ea.w[u] != 0) red_add(ta + ea.c[u], ea.w[u]);
+        if (gb < all) {
+            AccT* tb = target(rb);
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (eb.w[u] != 0) red_add(tb + eb.c[u], eb.w[u]);
+        }
+    }
+    // items beyond the stage, list by list
+    if (M > IT_BUF) {
+        for (int k = 0; k < nl; k++) {
+            const int64_t lo_j = max(off[k], (int64_t)IT_BUF), hi_j = off[k + 1];
+            if (lo_j >= hi_j) continue;
+            push_range<AccT, LANES>(N, S, a0 + k - 1, q, acc_slot<AccT>(N, S, a0 + k), s_pre + k * MAX_SEG,
+                                    g0[k] + (lo_j - off[k]), g0[k] + (hi_j - off[k]), ptid / LANES,
+                                    PUSH_THREADS / LANES, ptid % LANES, s_reset, s_stop, b0);
+        }
+    }
+    push_sync();                                 // the records are free again
+}
+
 // One launch runs `A.steps` steps of the instances [b0, b0 + G) (group q); the warp roles and the
 // bitmap rotation are described at the top of this file.
 template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD, int LANES>
@@ -389,12 +551,13 @@ __global__ void __launch_bounds__(PT, 1)
     uint32_t* maps = reinterpret_cast<uint32_t*>(smem + lay.kbits);
     uint8_t* sr = smem + lay.ref;            // bits 0-5 refractory, 6 plastic target, 7 nonzero bias
     uint8_t* s_active = smem + lay.misc;
-    int32_t* s_cnt = reinterpret_cast<int32_t*>(smem + lay.misc + 64);   // -, list cursor, push totals x2
+    int32_t* s_cnt = reinterpret_cast<int32_t*>(smem + lay.misc + 64);   // -, list cursor, push totals
     int32_t* s_scan = reinterpret_cast<int32_t*>(smem + lay.scan);
     int32_t* s_pre = reinterpret_cast<int32_t*>(smem + lay.pre);         // segment prefixes x2 (step parity)
     int32_t* s_spk = reinterpret_cast<int32_t*>(smem + lay.spk);
     int64_t* s_reset = reinterpret_cast<int64_t*>(smem + lay.ticks);     // per instance of the group
     int64_t* s_stop = s_reset + 64;
+    int4* s_items = reinterpret_cast<int4*>(smem + lay.items);
     const Lif<float> L = N.L32;
     const int n_ref = N.n_ref;
     const int tid = threadIdx.x;
@@ -429,7 +592,7 @@ __global__ void __launch_bounds__(PT, 1)
     if (tid == 0) {
         mbar_init(mbar, 1);
         fence_mbar_init();
-        for (int c = 0; c < 8; c++) s_cnt[c] = 0;
+        for (int c = 0; c < 16; c++) s_cnt[c] = 0;
     }
     if (tid < G) {                                               // the ticks stay constant during a launch
         s_reset[tid] = S.reset_tick[b0 + tid];
@@ -448,141 +611,152 @@ __global__ void __launch_bounds__(PT, 1)
     int32_t* err = S.err;
     const uint32_t acc_bytes = (uint32_t)cnt * (uint32_t)sizeof(AccT);
     const int32_t i0 = (int32_t)((lo + 4 * tid) % np), bl0 = (int32_t)((lo + 4 * tid) / np);
+    const int K = A.epoch;
+    const int64_t t_end = A.t0 + A.steps;
+    const bool is_u = tid < U_THREADS, is_p = !is_u && tid < U_THREADS + PUSH_THREADS;
+    const int ptid = tid - U_THREADS, lt = tid - U_THREADS - PUSH_THREADS;
+    int64_t pushed = A.pushed_until;                            // the arrivals of ticks < pushed are complete
     int32_t last = -1;                                          // step whose spikes still need listing
+    bool stop = false;
+    bool staged = false;                                        // this step's slice load was issued early
 
-    for (int32_t s = 0; s < A.steps; s++) {
-        const int64_t t = A.t0 + s;
-        const uint32_t step_no = A.step0 + (uint32_t)s;
-        const AccT* acc = reinterpret_cast<const AccT*>((t & 1) ? S.acc1 : S.acc0);
-        uint32_t* map = maps + (s % 3) * wpm;
-        if (tid == 0) stamp(A, s, 0);
-        // the accumulator slice of this step -> shared memory, one bulk load
-        if (tid == 0 && cnt > 0) {
-            fence_proxy_async_global();
-            mbar_expect_tx(mbar, acc_bytes);
-            for (uint32_t off = 0; off < acc_bytes; off += LOAD_PIECE)
-                tma_load_1d(reinterpret_cast<uint8_t*>(sacc) + off,
-                            reinterpret_cast<const uint8_t*>(acc + acc_base) + off, min((uint32_t)LOAD_PIECE, acc_bytes - off),
-                            mbar);
+    // ---- prologue: the arrivals of the first epoch not in the accumulators yet -----------------
+    if (A.steps > 0) {
+        const int64_t a1 = min(A.t0 + K, t_end + 1);
+        if (pushed < a1) {
+            if (is_p) push_arrivals<AccT, LANES>(N, S, q, b0, pushed, a1, s_pre, s_cnt, s_reset, s_stop, ptid);
+            barriers++;
+            stop = grid_barrier(A, barriers * gridDim.x, err, 1);
+            pushed = a1;
         }
-        if (tid < G) s_active[tid] = t < s_stop[tid];
-        // this CTA's segment consumed by the pushes at t-1 starts empty (the step engine appends to it)
-        if (tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q, blockIdx.x) = 0;
-        __syncthreads();
-        if (tid < U_THREADS) {
-            if (tid == 0) stamp(A, s, 1);
-            bool ok = true;
-            if (cnt > 0 && tid == 0) ok = stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
-            ok = !u_sync_or(!ok);        // one thread waited; every U thread agrees on the outcome
-            if (cnt > 0 && ok) (void)mbar_try_wait(mbar, (uint32_t)(s & 1));   // completed: acquire only
-            if (tid == 0) stamp(A, s, 2);
-            if (cnt > 0 && ok && tid == 0) {     // the slice is in shared memory: clear it in global memory
-                AccT* accw = const_cast<AccT*>(acc) + acc_base;
-                for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
-                    tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
-                bulk_commit();
-            }
-            // ---- advance every owned pair, four consecutive pairs per thread (a quad never straddles
-            //      two instances: rows are padded to 16); the step's kicks are read from the map and
-            //      its spikes written back into it --------------------------------------------------
-            if (ok) {
-                int32_t i = i0, bl = bl0;
-                const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
-                for (int32_t kb = 0; kb < cnt; kb += 4 * U_THREADS) {
-                    const int32_t k = kb + 4 * tid;
-                    const uint32_t kick4 = (map[k >> 5] >> sh) & 15u;
-                    uint32_t spk4 = 0;
-                    if (k < cnt && i < n && s_active[bl]) {
-                        const uint32_t fl = *reinterpret_cast<const uint32_t*>(sr + k);
-                        if ((fl & 0xc0c0c0c0u) == 0) {   // no plastic target, no bias: the common quad
-                            AccT x[4];
-                            load4(sacc + k, x);
-                            const float4 v4 = *reinterpret_cast<const float4*>(sv + k);
-                            const float4 g4 = *reinterpret_cast<const float4*>(sg + k);
-                            float vv[4] = {v4.x, v4.y, v4.z, v4.w}, gg[4] = {g4.x, g4.y, g4.z, g4.w};
-                            uint32_t ff = fl;
-#pragma unroll
-                            for (int j = 0; j < 4; j++) {
-                                if (i + j >= n) continue;
-                                int r = (int)((fl >> (8 * j)) & 0x3f);
-                                // the engine always fuses the two multiply-adds, as the shipped reference does
-                                if (lif_step<float>(vv[j], gg[j], r, acc_to_real<float>(x[j], L.w_syn), false, 0.0f,
-                                                    (kick4 >> j) & 1u, L, n_ref, true))
-                                    spk4 |= 1u << j;
-                                ff = (ff & ~(0xffu << (8 * j))) | ((uint32_t)r << (8 * j));
-                            }
-                            *reinterpret_cast<float4*>(sv + k) = make_float4(vv[0], vv[1], vv[2], vv[3]);
-                            *reinterpret_cast<float4*>(sg + k) = make_float4(gg[0], gg[1], gg[2], gg[3]);
-                            *reinterpret_cast<uint32_t*>(sr + k) = ff;
-                        } else {
-                            const int32_t b = b0 + bl;
-                            int64_t* pring_row =
-                                PLASTIC ? S.pring + (pos_mod(t, N.R) * N.B + b) * (int64_t)N.n_ppost : nullptr;
-                            spk4 = quad_special<AccT, PLASTIC>(sacc + k, sv + k, sg + k, sr + k, kick4, min(4, n - i),
-                                                               pring_row, N.ppost_of + i,
-                                                               S.bias_ext + (int64_t)b * S.n_ext, S.ext_idx + i, L, n_ref);
-                        }
-                    }
-                    // the 8 lanes of a 32-pair word OR their nibbles together; one of them stores it
-                    uint32_t word = spk4 << sh;
-                    word |= __shfl_xor_sync(0xffffffffu, word, 1);
-                    word |= __shfl_xor_sync(0xffffffffu, word, 2);
-                    word |= __shfl_xor_sync(0xffffffffu, word, 4);
-                    if ((lane & 7) == 0) map[k >> 5] = word;
-                    i += 4 * U_THREADS;
-                    while (i >= np) { i -= np; bl++; }
-                }
-            }
-            fence_proxy_async_shared();          // reads of the slice before the next bulk load
-            if (tid == 0) stamp(A, s, 3);
-            // ---- the next step's kicks (they depend on nothing this step computes) ----------------
-            if (s + 1 < A.steps)
-                kicks_into<RASTER>(N, S, A, maps + ((s + 1) % 3) * wpm, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1,
-                                   tid, U_THREADS, s_stop);
-            if (tid == 0) stamp(A, s, 4);
-        } else if (tid < U_THREADS + PUSH_THREADS) {
-            const int ptid = tid - U_THREADS;
-            if (ptid == 0) stamp(A, s, 7);
-            // ---- scatter the items that arrive at t+1 into the other accumulator -------------------
-            AccT* acc_next = reinterpret_cast<AccT*>(((t + 1) & 1) ? S.acc1 : S.acc0);
-            int32_t* pre = s_pre + (s & 1) * MAX_SEG;
-            if (t + 1 - N.n_delay >= 0) {
-                // the segment prefix of the list scattered now; with n_delay >= 4 the previous step
-                // computed it already (its counts were final one barrier earlier)
-                if (ptid < 32 && (s == 0 || N.n_delay < 4)) {
-                    const int32_t tot = segment_prefix(S, pos_mod(t + 1 - N.n_delay, N.R), q, pre);
-                    if (ptid == 0) s_cnt[2 + (s & 1)] = tot;
-                }
-                push_sync();
-                if (ptid == 0) stamp(A, s, 9);
-                const int64_t total = s_cnt[2 + (s & 1)];   // this CTA's share: a contiguous range of items
-                const int64_t g0 = total * blockIdx.x / gridDim.x, g1 = total * (blockIdx.x + 1) / gridDim.x;
-                push_range<AccT, LANES>(N, S, t, q, acc_next, pre, g0, g1, ptid / LANES, PUSH_THREADS / LANES,
-                                        ptid % LANES, s_reset, s_stop, b0);
-            }
-            // ---- the next step's segment prefix (its counts were written before this step began)
-            if (N.n_delay >= 4 && ptid < 32 && t + 2 - N.n_delay >= 0) {
-                const int32_t tot = segment_prefix(S, pos_mod(t + 2 - N.n_delay, N.R), q, s_pre + ((s + 1) & 1) * MAX_SEG);
-                if (ptid == 0) s_cnt[2 + ((s + 1) & 1)] = tot;
-            }
-            if (ptid == 0) stamp(A, s, 10);
+    }
+    // ---- epochs of K steps, one grid barrier each ---------------------------------------------
+    for (int32_t ep0 = 0; ep0 < A.steps && !stop; ep0 += K) {
+        const int32_t ep1 = min(ep0 + K, A.steps);
+        const int64_t te_end = A.t0 + ep1;
+        // pushes of this epoch: the arrivals of the next epoch (and of the tick after the run)
+        const int64_t pa0 = max(pushed, te_end), pa1 = min(te_end + K, t_end + 1);
+        if (is_p) {
+            if (ptid == 0) stamp(A, ep0, 7);
+            if (pa0 < pa1)
+                push_epoch<AccT, LANES>(N, S, q, b0, pa0, pa1, s_pre, s_cnt, s_scan + 16, s_items, s_reset, s_stop,
+                                        ptid);
+            if (ptid == 0) stamp(A, ep0, 10);
         } else {
-            // ---- the previous step's spikes: counts, plastic rows, work items ---------------------
-            const int lt = tid - U_THREADS - PUSH_THREADS;
-            if (s >= 1)
-                list_spikes<PLASTIC, RECORD>(N, S, A, maps + ((s - 1) % 3) * wpm, s - 1, t - 1, b0, q, lo, used_words,
-                                             s_cnt, s_scan, s_spk, lt, LIST_THREADS, []() { list_sync(); });
-            if (lt == 0) stamp(A, s, 8);
+            for (int32_t s = ep0; s < ep1; s++) {
+                const int64_t t = A.t0 + s;
+                const uint32_t step_no = A.step0 + (uint32_t)s;
+                const AccT* acc = acc_slot<AccT>(N, S, t);
+                uint32_t* map = maps + (s % 3) * wpm;
+                ul_sync();                       // neuron and listing warps: step boundary
+                if (is_u) {
+                    if (tid == 0) stamp(A, s, 0);
+                    if (tid == 0 && cnt > 0 && !staged && !ld_volatile_i32(A.abort_flag))
+                        issue_slice(acc + acc_base, sacc, acc_bytes, mbar);
+                    if (tid < G) s_active[tid] = t < s_stop[tid];
+                    // this CTA's list segment consumed by the pushes for tick t starts empty (the
+                    // step engine appends to it)
+                    if (tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q, blockIdx.x) = 0;
+                    if (tid == 0) stamp(A, s, 1);
+                    bool ok = true;
+                    if (cnt > 0 && tid == 0)
+                        ok = !ld_volatile_i32(A.abort_flag) && stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
+                    ok = !u_sync_or(!ok);        // one thread waited; every U thread agrees on the outcome
+                    if (cnt > 0 && ok) (void)mbar_try_wait(mbar, (uint32_t)(s & 1));   // completed: acquire only
+                    if (tid == 0) stamp(A, s, 2);
+                    if (cnt > 0 && ok && tid == 0) {     // the slice is in shared memory: clear it in global memory
+                        AccT* accw = const_cast<AccT*>(acc) + acc_base;
+                        for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
+                            tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
+                        bulk_commit();
+                    }
+                // ---- advance every owned pair, four consecutive pairs per thread (a quad never straddles
+                //      two instances: rows are padded to 16); the step's kicks are read from the map and
+                //      its spikes written back into it --------------------------------------------------
+                if (ok) {
+                    int32_t i = i0, bl = bl0;
+                    const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
+                    for (int32_t kb = 0; kb < cnt; kb += 4 * U_THREADS) {
+                        const int32_t k = kb + 4 * tid;
+                        const uint32_t kick4 = (map[k >> 5] >> sh) & 15u;
+                        uint32_t spk4 = 0;
+                        if (k < cnt && i < n && s_active[bl]) {
+                            const uint32_t fl = *reinterpret_cast<const uint32_t*>(sr + k);
+                            if ((fl & 0xc0c0c0c0u) == 0) {   // no plastic target, no bias: the common quad
+                                AccT x[4];
+                                load4(sacc + k, x);
+                                const float4 v4 = *reinterpret_cast<const float4*>(sv + k);
+                                const float4 g4 = *reinterpret_cast<const float4*>(sg + k);
+                                float vv[4] = {v4.x, v4.y, v4.z, v4.w}, gg[4] = {g4.x, g4.y, g4.z, g4.w};
+                                uint32_t ff = fl;
+    #pragma unroll
+                                for (int j = 0; j < 4; j++) {
+                                    if (i + j >= n) continue;
+                                    int r = (int)((fl >> (8 * j)) & 0x3f);
+                                    // the engine always fuses the two multiply-adds, as the shipped reference does
+                                    if (lif_step<float>(vv[j], gg[j], r, acc_to_real<float>(x[j], L.w_syn), false, 0.0f,
+                                                        (kick4 >> j) & 1u, L, n_ref, true))
+                                        spk4 |= 1u << j;
+                                    ff = (ff & ~(0xffu << (8 * j))) | ((uint32_t)r << (8 * j));
+                                }
+                                *reinterpret_cast<float4*>(sv + k) = make_float4(vv[0], vv[1], vv[2], vv[3]);
+                                *reinterpret_cast<float4*>(sg + k) = make_float4(gg[0], gg[1], gg[2], gg[3]);
+                                *reinterpret_cast<uint32_t*>(sr + k) = ff;
+                            } else {
+                                const int32_t b = b0 + bl;
+                                int64_t* pring_row =
+                                    PLASTIC ? S.pring + (pos_mod(t, N.R_pl) * N.B + b) * (int64_t)N.n_ppost : nullptr;
+                                spk4 = quad_special<AccT, PLASTIC>(sacc + k, sv + k, sg + k, sr + k, kick4, min(4, n - i),
+                                                                   pring_row, N.ppost_of + i,
+                                                                   S.bias_ext + (int64_t)b * S.n_ext, S.ext_idx + i, L, n_ref);
+                            }
+                        }
+                        // the 8 lanes of a 32-pair word OR their nibbles together; one of them stores it
+                        uint32_t word = spk4 << sh;
+                        word |= __shfl_xor_sync(0xffffffffu, word, 1);
+                        word |= __shfl_xor_sync(0xffffffffu, word, 2);
+                        word |= __shfl_xor_sync(0xffffffffu, word, 4);
+                        if ((lane & 7) == 0) map[k >> 5] = word;
+                        i += 4 * U_THREADS;
+                        while (i >= np) { i -= np; bl++; }
+                    }
+                }
+
+                    fence_proxy_async_shared();      // reads of the slice before the next bulk load
+                    // the next step's slice, when it lies in this epoch (its arrivals are complete),
+                    // loads while the kicks are drawn
+                    staged = ok && s + 1 < ep1;
+                    if (staged) {
+                        u_sync();
+                        if (tid == 0 && cnt > 0) issue_slice(acc_slot<AccT>(N, S, t + 1) + acc_base, sacc, acc_bytes, mbar);
+                    }
+                    if (tid == 0) stamp(A, s, 3);
+                    // ---- the next step's kicks (they depend on nothing this step computes) --------
+                    if (s + 1 < A.steps)
+                        kicks_into<RASTER>(N, S, A, maps + ((s + 1) % 3) * wpm, s + 1, t + 1, step_no + 1u, b0, G, lo, e0,
+                                           e1, tid, U_THREADS, s_stop);
+                    if (tid == 0) stamp(A, s, 4);
+                } else {
+                    // ---- the previous step's spikes: counts, plastic rows, work items -------------
+                    if (s >= 1)
+                        list_spikes<PLASTIC, RECORD>(N, S, A, maps + ((s - 1) % 3) * wpm, s - 1, t - 1, b0, q, lo,
+                                                     used_words, s_cnt, s_scan, s_spk, lt, LIST_THREADS,
+                                                     []() { list_sync(); });
+                    if (lt == 0) stamp(A, s, 8);
+                }
+            }
         }
+        pushed = max(pushed, pa1);
+        staged = false;
         if (tid == 0 && cnt > 0) {
-            bulk_wait_all();                     // the cleared slice is written before anyone pushes into it
+            bulk_wait_all();                     // the cleared slices are written before anyone pushes into them
             fence_proxy_async_global();
         }
-        if (tid == 0) stamp(A, s, 5);
+        if (tid == 0) stamp(A, ep1 - 1, 5);
         barriers++;
-        last = s;
-        if (grid_barrier(A, barriers * gridDim.x, err, s + 1)) { last = -1; break; }
-        if (tid == 0) stamp(A, s, 6);
+        last = ep1 - 1;
+        if (grid_barrier(A, barriers * gridDim.x, err, ep1 + 1)) { last = -1; stop = true; break; }
+        if (tid == 0) stamp(A, ep1 - 1, 6);
     }
     if (tid == 0) bulk_wait_all();
     // the last step's spikes are listed before the launch ends (the next launch scatters them)

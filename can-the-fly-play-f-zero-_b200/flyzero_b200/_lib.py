@@ -36,7 +36,7 @@ class Info(C.Structure):
                 ("propagation", C.c_int32), ("lanes", C.c_int32), ("group", C.c_int32), ("ctas", C.c_int32),
                 ("n_plastic", C.c_int64), ("n_ext", C.c_int64), ("t", C.c_int64), ("step_no", C.c_uint32),
                 ("launches", C.c_int64), ("item_capacity", C.c_int64), ("bytes_device", C.c_int64),
-                ("decay_syn", C.c_double), ("decay_m", C.c_double), ("kick", C.c_double)]
+                ("decay_syn", C.c_double), ("decay_m", C.c_double), ("kick", C.c_double), ("epoch", C.c_int32)]
 
 
 class Views(C.Structure):

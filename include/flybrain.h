@@ -73,6 +73,7 @@ typedef struct {
     double decay_syn;     /* exp(-dt / tau_syn), computed in FP64 on the device */
     double decay_m;       /* dt / tau_m */
     double kick;          /* f_poisson * w_syn, mV */
+    int32_t epoch;        /* persistent engine: steps between grid barriers (accumulator slots = 2x) */
 } fb_info;
 
 /* Device views of the mutable state a caller may read and write between runs. */
@@ -159,10 +160,11 @@ int fb_reward_step(fb_brain* brain, const int32_t* counts, double* elig, float* 
 int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
 
 /* Phase trace of the persistent engine (diagnostics). `trace` [device] holds `capacity` int64;
- * every later fb_run whose steps * ctas * 11 fits records, per step and CTA, the SM clock at 11
- * points: step start, neuron warps start, accumulator slice staged, neurons advanced, next kicks
- * done, barrier arrival (neuron warps), barrier exit, push warps start, listing warps done, push
- * warps' segment prefix ready, push warps done. NULL: off. No counterpart in the reference. */
+ * every later fb_run whose steps * ctas * 11 fits records, per step and CTA, the SM clock at
+ * these points: 0 step start, 1 accumulator slice requested, 2 slice staged, 3 neurons advanced,
+ * 4 next kicks drawn, 8 listing warps done; per epoch of steps between grid barriers, at its first
+ * step 7 push warps start and 10 push warps done, at its last step 5 grid-barrier arrival and
+ * 6 grid-barrier exit. NULL: off. No counterpart in the reference. */
 int fb_set_trace(fb_brain* brain, long long* trace, int64_t capacity);
 
 /* Device error flags raised since the last call (overflow, barrier timeout), then cleared.
