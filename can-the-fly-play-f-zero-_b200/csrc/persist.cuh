@@ -35,7 +35,8 @@ constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulato
 constexpr int SPK_BUF = 1024;           // spikes of one CTA and step listed in parallel
 constexpr int IT_BUF = 384;             // work items of one CTA's epoch push staged in shared memory
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
-constexpr int MAX_EPOCH = 8;            // steps per epoch at most (accumulator slots: twice that)
+constexpr int MAX_EPOCH = 4;            // steps per epoch at most (accumulator slots: twice that; 8 slots of a
+                                        // 16-instance group stay in L2, which measured faster than longer epochs)
 
 constexpr int PUSH_WARPS = 4;                              // warps that scatter arriving items ...
 constexpr int LIST_WARPS = 2;                              // ... that list the previous step's spikes ...
