@@ -141,6 +141,172 @@ __global__ void __launch_bounds__(256) k_gemm(const uint16_t* __restrict__ A, co
         }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The same GEMM on the 5th-generation tensor cores: tcgen05.mma (kind::f16, BF16 in, FP32
+// accumulate) issued by one thread, operands in shared memory in the K-major no-swizzle
+// core-matrix layout (8 rows x 16 bytes per core matrix), the 128 x BN accumulator in tensor memory
+// (TMEM), read back with tcgen05.ld for the fused epilogue. Four shared-memory stages filled by
+// cp.async: later K tiles load while the tensor cores work on the current one (a stage is
+// refilled once tcgen05.commit's mbarrier shows its MMAs done).
+// ---------------------------------------------------------------------------------------------
+constexpr int TC_BM = 128, TC_BK = 64, TC_THREADS = 128, TC_STAGES = 4;
+constexpr long long TC_WAIT_CYCLES = 4000000000LL;            // bounded waits (~2 s)
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: K-major, no swizzle; lbo = byte distance between the two 8-column
+// halves of a K=16 slice, sbo = byte distance between 8-row groups
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);   // version 1, base offset 0, no swizzle
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    uint32_t done = 0;
+    while (!done) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(mbar), "r"(parity)
+            : "memory");
+        if (!done && clock64() - t0 > TC_WAIT_CYCLES) return false;
+    }
+    return true;
+}
+
+// 16-byte global -> shared copy without a register round trip (zero-filled outside the matrix)
+__device__ __forceinline__ void cp_async16(void* dst, const uint16_t* X, int row, int k, int rows, int K, int ld)
+{
+    if (row < rows && k + 8 <= K) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(su32(dst)), "l"(X + (int64_t)row * ld + k)
+                     : "memory");
+    } else {
+        uint16_t tmp[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) tmp[u] = (row < rows && k + u < K) ? X[(int64_t)row * ld + k + u] : (uint16_t)0;
+        *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(tmp);
+    }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(const uint16_t* __restrict__ A, const uint16_t* __restrict__ B,
+                                                         int M, int N, int K, int lda, int ldb, Epi e)
+{
+    constexpr int A_BYTES = TC_BM * TC_BK * 2, B_BYTES = BN * TC_BK * 2, STAGE = A_BYTES + B_BYTES;
+    constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+    extern __shared__ __align__(1024) uint8_t sm[];
+    __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&s_tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < TC_STAGES; s++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&mbar[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    // instruction descriptor: FP32 accumulate (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1),
+    // both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+    const int nk = (K + TC_BK - 1) / TC_BK;
+    // one K tile -> stage st: 16-byte chunks (row r, k-chunk kc) in the core-matrix layout
+    auto load_tile = [&](int kt) {
+        uint8_t* sa = sm + (kt % TC_STAGES) * STAGE;
+        uint8_t* sb = sa + A_BYTES;
+        const int k0 = kt * TC_BK;
+        for (int c = tid; c < TC_BM * 8; c += TC_THREADS) {
+            const int r = c >> 3, kc = c & 7;
+            cp_async16(sa + (kc * TC_BM + r) * 16, A, m0 + r, k0 + kc * 8, M, K, lda);
+        }
+        for (int c = tid; c < BN * 8; c += TC_THREADS) {
+            const int r = c >> 3, kc = c & 7;
+            cp_async16(sb + (kc * BN + r) * 16, B, n0 + r, k0 + kc * 8, N, K, ldb);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    bool ok = true;
+    for (int kt = 0; kt < TC_STAGES - 1; kt++) {
+        if (kt < nk) load_tile(kt);
+        else asm volatile("cp.async.commit_group;" ::: "memory");        // keep the group count uniform
+    }
+    for (int kt = 0; kt < nk; kt++) {
+        const int st = kt % TC_STAGES;
+        asm volatile("cp.async.wait_group %0;" ::"n"(TC_STAGES - 2) : "memory");   // tile kt has landed
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");      // generic writes -> tensor-core reads
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint8_t* sa = sm + st * STAGE;
+            uint8_t* sb = sa + A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TC_BK / 16; kk++) {
+                const uint64_t ad = smem_desc(su32(sa) + kk * 2 * TC_BM * 16, TC_BM * 16, 128);
+                const uint64_t bd = smem_desc(su32(sb) + kk * 2 * BN * 16, BN * 16, 128);
+                const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             su32(&mbar[st]))
+                         : "memory");
+        }
+        // refill the stage the previous tile used once its MMAs are done
+        const int nxt = kt + TC_STAGES - 1;
+        if (nxt < nk) {
+            if (kt >= 1) {
+                const int ps = (kt - 1) % TC_STAGES;
+                ok = tc_wait(su32(&mbar[ps]), (uint32_t)(((kt - 1) / TC_STAGES) & 1)) && ok;
+            }
+            load_tile(nxt);
+        } else {
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        }
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+    // the last commit covers every MMA issued before it
+    ok = tc_wait(su32(&mbar[(nk - 1) % TC_STAGES]), (uint32_t)(((nk - 1) / TC_STAGES) & 1)) && ok;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // epilogue: warp w holds rows 32w..32w+31 (TMEM lanes), 16 columns per load
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(addr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) epilogue(e, M, N, row, n0 + c0 + j, __uint_as_float(v[j]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
 __global__ void k_poisson(const float* z, const float* y, int M, int D, double* loss, uint16_t* dz, int ldd, uint16_t* dz_t)
 {
     __shared__ double part[8];
@@ -206,6 +372,8 @@ __global__ void k_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* ou
     }
 }
 
+int g_gemm_kind = FS_GEMM_TCGEN05;
+
 int fail(const char* msg)
 {
     fb::set_last_error(msg);
@@ -218,6 +386,21 @@ int cuda_status()
     if (e == cudaSuccess) return FB_OK;
     fb::set_last_error(cudaGetErrorString(e));
     return FB_ERR_CUDA;
+}
+
+template <int BN>
+int launch_tc(const uint16_t* A, const uint16_t* B, int M, int N, int K, int lda, int ldb, const Epi& e, cudaStream_t st)
+{
+    constexpr int smem = TC_STAGES * (TC_BM * TC_BK * 2 + BN * TC_BK * 2);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return cuda_status();
+        attr = true;
+    }
+    dim3 grid((N + BN - 1) / BN, (M + TC_BM - 1) / TC_BM);
+    k_gemm_tc<BN><<<grid, TC_THREADS, smem, st>>>(A, B, M, N, K, lda, ldb, e);
+    return cuda_status();
 }
 
 unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
@@ -237,9 +420,22 @@ extern "C" int fs_gemm(const uint16_t* A, const uint16_t* B, int32_t M, int32_t 
     if ((epi == FS_EPI_BIAS_GELU || epi == FS_EPI_GELU_GRAD) && !out_bf16) return fail("fs_gemm: out_bf16 needed");
     if (epi == FS_EPI_GELU_GRAD && !zin) return fail("fs_gemm: zin needed");
     Epi e{epi, ldo, ldo_t, bias, zin, out_f32, out_bf16, out_bf16_t};
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g_gemm_kind == FS_GEMM_TCGEN05) {
+        if (N <= 16) return launch_tc<16>(A, B, M, N, K, lda, ldb, e, st);
+        return launch_tc<64>(A, B, M, N, K, lda, ldb, e, st);
+    }
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    k_gemm<<<grid, 256, 0, (cudaStream_t)stream>>>(A, B, M, N, K, lda, ldb, e);
+    k_gemm<<<grid, 256, 0, st>>>(A, B, M, N, K, lda, ldb, e);
     return cuda_status();
+}
+
+extern "C" int fs_gemm_kind(int32_t kind)
+{
+    if (kind != FS_GEMM_MMA_SYNC && kind != FS_GEMM_TCGEN05 && kind != -1) return fail("fs_gemm_kind: unknown kind");
+    const int old = g_gemm_kind;
+    if (kind >= 0) g_gemm_kind = kind;
+    return old;
 }
 
 extern "C" int fs_poisson_nll(const float* z, const float* y, int32_t M, int32_t D, double* loss_sum, uint16_t* dz,

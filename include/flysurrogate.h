@@ -26,6 +26,14 @@ extern "C" {
 #define FS_EPI_BIAS_F32 2     /* out_f32 = C + bias[j] */
 #define FS_EPI_GELU_GRAD 3    /* d = C * gelu'(zin[i][j]) -> out_bf16, transpose -> out_bf16_t */
 
+/* GEMM kinds: the BF16 m16n8k16 warp MMA, or tcgen05 (one thread issues 128 x N x 16 tensor-core
+ * MMAs from shared-memory descriptors, FP32 accumulator in tensor memory); default tcgen05. */
+#define FS_GEMM_MMA_SYNC 0
+#define FS_GEMM_TCGEN05 1
+
+/* Select the kind fs_gemm uses (-1: keep); returns the previous kind. */
+int fs_gemm_kind(int32_t kind);
+
 /* C[M x N] = A[M x K] * B[N x K]^T with bf16 A (row stride lda), bf16 B (row stride ldb), FP32
  * accumulation, then the epilogue `epi` writing rows of stride ldo (transposed outputs: stride
  * ldo_t). Any M, N, K >= 1; lda, ldb multiples of 8. */

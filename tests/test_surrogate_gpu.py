@@ -24,11 +24,14 @@ def _p(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
+@pytest.mark.parametrize("kind", [1, 0], ids=["tcgen05", "mma_sync"])
 @pytest.mark.parametrize("M,N,K", [(300, 70, 200), (128, 64, 32), (37, 10, 16), (4096, 512, 1280)])
-def test_gemm_and_epilogues_match_torch_fp32(torch, M, N, K):
+def test_gemm_and_epilogues_match_torch_fp32(torch, M, N, K, kind):
+    """Both GEMM kinds (tcgen05 with the accumulator in tensor memory, and the warp MMA)."""
     from flyzero_b200 import _lib
 
     L = _lib.load()
+    old = L.fs_gemm_kind(kind)
     g = torch.Generator(device="cuda").manual_seed(M + N + K)
     A = torch.randn((M, K), device="cuda", generator=g).to(torch.bfloat16)
     B = torch.randn((N, K), device="cuda", generator=g).to(torch.bfloat16)
@@ -54,6 +57,7 @@ def test_gemm_and_epilogues_match_torch_fp32(torch, M, N, K):
     zz = zin.clone().requires_grad_(True)
     torch.nn.functional.gelu(zz).backward(ref)
     torch.testing.assert_close(d.float(), zz.grad, rtol=1e-2, atol=1e-2 * float(ref.abs().max()))
+    L.fs_gemm_kind(old)
 
 
 def test_training_gradients_match_fp64_oracle(torch):
