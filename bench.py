@@ -130,26 +130,32 @@ def barrier(world):
         dist.barrier()
 
 
-def max_over_ranks(x: float, world: int) -> float:
+def _reduce(x: float, world: int, op: str, device: str) -> float:
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
 
 
-def sum_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The slowest rank's time (replicas report the job's wall time as the max over ranks)."""
+    return _reduce(x, world, "max", device)
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+
+def sum_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    return _reduce(x, world, "sum", device)
+
+
+def replica_value(neuron_steps: float, elapsed_ms: float, world: int, device: str = "cuda") -> tuple:
+    """Whole-job throughput of independent replicas: all ranks' neuron-steps over the slowest
+    rank's device time. Returns (value, max_ms)."""
+    total = sum_over_ranks(float(neuron_steps), world, device)
+    max_ms = max_over_ranks(float(elapsed_ms), world, device)
+    return total / (max_ms / 1000.0), max_ms
 
 
 def workload(batch: int, seed: int):
@@ -315,9 +321,7 @@ def run_ours(args, world, rank, local):
     stop = (work.run_ms / DT).astype(np.int64)
     active = int(sum(np.clip(stop - (t0 + k * fs), 0, fs).sum() for k in range(args.steps)))
     neuron_steps = active * n
-    total_ns = sum_over_ranks(float(neuron_steps), world)
-    max_ms = max_over_ranks(elapsed_ms, world)
-    value = total_ns / (max_ms / 1000.0)
+    value, max_ms = replica_value(neuron_steps, elapsed_ms, world)
     spk, edges = spike_bytes(counts[args.warmup:], rowlen)
     alg_bytes = BYTES_PER_NEURON_STEP * neuron_steps + BYTES_PER_SPIKE * spk + BYTES_PER_EDGE * edges
     info = gb.info()
