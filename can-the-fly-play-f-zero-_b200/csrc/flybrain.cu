@@ -14,6 +14,7 @@
 #include "host_prep.hpp"
 #include "persist.cuh"
 #include "plastic.cuh"
+#include "readout.cuh"
 
 using namespace fb;
 
@@ -611,6 +612,34 @@ extern "C" int fb_reward_step(fb_brain* h, const int32_t* counts, double* elig, 
     k_reward_post_mean<<<(unsigned)((np_ + 255) / 256), 256, 0, st>>>(a);
     CU(cudaGetLastError());
     h->launches += 2;
+    return FB_OK;
+}
+
+extern "C" int fb_group_rates(const fb_brain* h, const int32_t* counts, const int32_t* idx, const int32_t* grp_ptr,
+                              int32_t n_groups, const float* w, float a, float hz, float* rates, void* stream)
+{
+    if (!h || !counts || !idx || !grp_ptr || !w || !rates || n_groups <= 0) return fail(FB_ERR_ARG, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    GroupArgs g{h->B, n_groups, h->n, counts, idx, grp_ptr};
+    const int64_t work = (int64_t)h->B * n_groups;
+    k_group_rates<<<(unsigned)((work + 127) / 128), 128, 0, (cudaStream_t)stream>>>(g, w, a, hz, rates);
+    CU(cudaGetLastError());
+    return FB_OK;
+}
+
+extern "C" int fb_clamp(fb_brain* h, const int32_t* counts, const int32_t* idx, const int32_t* grp_ptr, int32_t n_groups,
+                        const int32_t* slot, const float* base, double a, double hz, float gain, float limit,
+                        float* rate, float* u, const float* target, const uint8_t* active, const float* gate,
+                        void* stream)
+{
+    if (!h || !counts || !idx || !grp_ptr || !slot || !base || !rate || !u || !target || !active || n_groups <= 0)
+        return fail(FB_ERR_ARG, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    GroupArgs g{h->B, n_groups, h->n, counts, idx, grp_ptr};
+    ClampArgs c{a, hz, gain, limit, rate, u, target, active, gate, slot, base, h->bias_ext, (int32_t)h->n_ext};
+    const int64_t work = (int64_t)h->B * n_groups;
+    k_clamp<<<(unsigned)((work + 127) / 128), 128, 0, (cudaStream_t)stream>>>(g, c);
+    CU(cudaGetLastError());
     return FB_OK;
 }
 

@@ -156,6 +156,24 @@ int fb_reward_step(fb_brain* brain, const int32_t* counts, double* elig, float* 
                    const int32_t* fly_ptr, const int32_t* fly_slots, const float* fly_weight, int32_t n_flies,
                    const uint8_t* mask, double ae, double ap, float cap, int32_t apply, void* stream);
 
+/* Frame-end readout of neuron groups (BatchMotor.update, flyzero/batch.py:105-109): for every
+ * instance b and group g (neurons idx[grp_ptr[g] .. grp_ptr[g+1]) [device]),
+ *   inst = f32(sum of counts[b][idx]) * w[g] * hz;  rates[b][g] += a * (inst - rates[b][g])
+ * counts [device] (batch, n); w [device] (n_groups) = 1 / group size; rates [device] (batch,
+ * n_groups) float32, updated in place. */
+int fb_group_rates(const fb_brain* brain, const int32_t* counts, const int32_t* idx, const int32_t* grp_ptr,
+                   int32_t n_groups, const float* w, float a, float hz, float* rates, void* stream);
+
+/* Closed-loop clamp of neuron groups (Clamp.step, flyzero/implant.py:84-104), all on the device:
+ *   rate = rate + a * (mean count * hz - rate);  on = active[b] * gate[b][g] (gate NULL: 1)
+ *   u = clip(u + gain * (target - rate) * on, -limit, limit) * active[b]
+ *   bias_ext[b][slot[k]] = base[b][k] + u * on     for every entry k of the group
+ * slot [device] ext slot of every idx entry; base [device] (batch, len(idx)); rate, u, target,
+ * gate [device] (batch, n_groups) float32; active [device] (batch) uint8. */
+int fb_clamp(fb_brain* brain, const int32_t* counts, const int32_t* idx, const int32_t* grp_ptr, int32_t n_groups,
+             const int32_t* slot, const float* base, double a, double hz, float gain, float limit, float* rate,
+             float* u, const float* target, const uint8_t* active, const float* gate, void* stream);
+
 /* Choose the schedule (FB_ENGINE_*, FB_PROP_*, lanes per work item 8/16/32; 0 keeps a field). */
 int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
 
