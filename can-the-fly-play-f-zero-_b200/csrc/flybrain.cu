@@ -15,6 +15,7 @@
 #include "persist.cuh"
 #include "plastic.cuh"
 #include "readout.cuh"
+#include "instruct.cuh"
 
 using namespace fb;
 
@@ -639,6 +640,56 @@ extern "C" int fb_clamp(fb_brain* h, const int32_t* counts, const int32_t* idx, 
     ClampArgs c{a, hz, gain, limit, rate, u, target, active, gate, slot, base, h->bias_ext, (int32_t)h->n_ext};
     const int64_t work = (int64_t)h->B * n_groups;
     k_clamp<<<(unsigned)((work + 127) / 128), 128, 0, (cudaStream_t)stream>>>(g, c);
+    CU(cudaGetLastError());
+    return FB_OK;
+}
+
+extern "C" int fb_trace_rates(const fb_brain* h, const int32_t* counts, const int32_t* upre, int32_t n_upre, float* trace,
+                              float a_pre, float scale_pre, const int32_t* upost, int32_t n_upost, float* rate,
+                              float a_rate, float hz, void* stream)
+{
+    if (!h || !counts || (n_upre > 0 && (!upre || !trace)) || (n_upost > 0 && (!upost || !rate)) || n_upre < 0 ||
+        n_upost < 0)
+        return fail(FB_ERR_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    const int64_t work = (int64_t)h->B * (n_upre + n_upost);
+    if (work == 0) return FB_OK;
+    const int blocks = (int)std::min<int64_t>((work + 255) / 256, (int64_t)h->sm_count * 8);
+    k_trace_rates<<<blocks, 256, 0, (cudaStream_t)stream>>>(counts, h->n, h->B, upre, n_upre, trace, a_pre, scale_pre,
+                                                            upost, n_upost, rate, a_rate, hz);
+    CU(cudaGetLastError());
+    return FB_OK;
+}
+
+extern "C" int fb_delta_apply(fb_brain* h, const int32_t* sel, const int32_t* pre_k, const int32_t* post_x, int32_t n_sel,
+                              const float* trace, int32_t n_tr, const float* x, int32_t n_x, const float* coef,
+                              const int32_t* fly_ptr, const int32_t* fly_slots, int32_t n_flies, const float* sign,
+                              const float* wmax, void* stream)
+{
+    if (!h || n_sel < 0 || n_flies <= 0) return fail(FB_ERR_ARG, "bad arguments");
+    if (n_sel == 0) return FB_OK;
+    if (!sel || !pre_k || !post_x || !trace || !x || !coef || !fly_ptr || !fly_slots || !sign || !wmax)
+        return fail(FB_ERR_ARG, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    DeltaArgs a{h->B, n_flies, n_sel, n_tr, n_x, h->n_pl, sel, pre_k, post_x, trace, x, coef, fly_ptr, fly_slots, sign,
+                wmax, h->pw};
+    const int64_t work = (int64_t)n_sel * n_flies;
+    k_delta_apply<<<(unsigned)((work + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a);
+    CU(cudaGetLastError());
+    return FB_OK;
+}
+
+extern "C" int fb_backprop(const fb_brain* h, const int32_t* sel, const int32_t* pre_l, const int32_t* post_x, int32_t n_sel,
+                           const float* x, int32_t n_x, float* delta, int32_t n_delta, void* stream)
+{
+    if (!h || n_sel < 0) return fail(FB_ERR_ARG, "bad arguments");
+    if (n_sel == 0) return FB_OK;
+    if (!sel || !pre_l || !post_x || !x || !delta) return fail(FB_ERR_ARG, "NULL argument");
+    CU(cudaSetDevice(h->device));
+    const int64_t work = (int64_t)h->B * n_sel;
+    const int blocks = (int)std::min<int64_t>((work + 255) / 256, (int64_t)h->sm_count * 8);
+    k_backprop<<<blocks, 256, 0, (cudaStream_t)stream>>>(h->B, n_sel, sel, pre_l, post_x, x, n_x, h->pw, h->n_pl,
+                                                         (float)h->params.w_syn, delta, n_delta);
     CU(cudaGetLastError());
     return FB_OK;
 }

@@ -174,6 +174,29 @@ int fb_clamp(fb_brain* brain, const int32_t* counts, const int32_t* idx, const i
              const int32_t* slot, const float* base, double a, double hz, float gain, float limit, float* rate,
              float* u, const float* target, const uint8_t* active, const float* gate, void* stream);
 
+/* Instructed plasticity, frame-end pieces (BatchInstruct / BatchInstructDeep / BatchInstructDeep2,
+ * flyzero/batch.py:226-451); every pointer [device], float32 state updated in place.
+ * fb_trace_rates: trace[b][k] += a_pre * (counts[b][upre[k]] * scale_pre - trace[b][k]) and
+ *   rate[b][k] += a_rate * (counts[b][upost[k]] * hz - rate[b][k])  (batch.py:282-287). */
+int fb_trace_rates(const fb_brain* brain, const int32_t* counts, const int32_t* upre, int32_t n_upre, float* trace,
+                   float a_pre, float scale_pre, const int32_t* upost, int32_t n_upost, float* rate, float a_rate,
+                   float hz, void* stream);
+
+/* fb_delta_apply: for the plastic entries sel[s] (s < n_sel), per fly f (slots
+ * fly_slots[fly_ptr[f] .. fly_ptr[f+1])): d = sum over its slots of coef[b] * trace[b][pre_k[s]] *
+ * x[b][post_x[s]], then every slot of the fly w = sign * clip(sign * (w + d), 0, wmax) on the
+ * engine's pw (the per-fly averaged delta rule, batch.py:158-172, 312-314, and the fused
+ * deep_update kernel, batch.py:26-51). */
+int fb_delta_apply(fb_brain* brain, const int32_t* sel, const int32_t* pre_k, const int32_t* post_x, int32_t n_sel,
+                   const float* trace, int32_t n_tr, const float* x, int32_t n_x, const float* coef,
+                   const int32_t* fly_ptr, const int32_t* fly_slots, int32_t n_flies, const float* sign,
+                   const float* wmax, void* stream);
+
+/* fb_backprop: delta[b][pre_l[s]] += (pw[b][sel[s]] / w_syn) * x[b][post_x[s]] (the retrograde
+ * error through the fly's own synapses, batch.py:390-393, 440-442; float atomics). */
+int fb_backprop(const fb_brain* brain, const int32_t* sel, const int32_t* pre_l, const int32_t* post_x, int32_t n_sel,
+                const float* x, int32_t n_x, float* delta, int32_t n_delta, void* stream);
+
 /* Choose the schedule (FB_ENGINE_*, FB_PROP_*, lanes per work item 8/16/32; 0 keeps a field). */
 int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
 
