@@ -35,6 +35,18 @@ def plastic_positions(conn, types=PLASTIC_TYPES) -> np.ndarray:
     return np.flatnonzero(is_t[w.indices])
 
 
+def save_state(path, st: dict):
+    """Plastic weights of one fly as the reference stores them: an npz with ``pos`` (CSR
+    positions), ``data`` (weights, mV), ``w0`` and, with intrinsic plasticity, ``bias_idx`` /
+    ``bias`` (flyzero/batch.py:195-219)."""
+    np.savez(path, **{k: np.asarray(v) for k, v in st.items()})
+
+
+def load_state(path) -> dict:
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
 def _ptr(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 

@@ -126,3 +126,81 @@ def csr_checksum(w: sp.csr_matrix) -> str:
     for a in (np.asarray(w.indptr, np.int64), np.asarray(w.indices, np.int32), np.asarray(w.data, np.float32)):
         h.update(np.ascontiguousarray(a).tobytes())
     return h.hexdigest()
+
+
+# ---- FlyWire v783 files (flyzero/connectome.py:123-165 reads the same three) ----------------
+FLYWIRE_FILES = ("Completeness_783.csv", "Connectivity_783.parquet", "neuron_annotations.tsv")
+_ANNOT_COLUMNS = ("super_class", "cell_class", "cell_type", "hemibrain_type", "side", "top_nt",
+                  "pos_x", "pos_y", "pos_z")
+
+
+@dataclass
+class Connectome:
+    """A connectome with its neuron table: ``weights`` (pre x post CSR, float32 signed synapse
+    counts) and ``neurons`` (one row per neuron in index order, with ``root_id``, ``cell_type``,
+    ``hemibrain_type``, ``side`` ... as in flyzero/connectome.py:68-82)."""
+
+    weights: sp.csr_matrix
+    neurons: object                        # pandas.DataFrame
+    name: str = "connectome"
+    _type_cache: dict = field(default_factory=dict, repr=False)
+
+    @property
+    def n(self) -> int:
+        return self.weights.shape[0]
+
+    @property
+    def nnz(self) -> int:
+        return self.weights.nnz
+
+    def find(self, cell_type: str, side: str | None = None) -> np.ndarray:
+        """Neurons whose cell type (or hemibrain type) equals ``cell_type`` (case-insensitive); a
+        trailing ``*`` matches a prefix (``DNg02*``). ``side`` filters by hemisphere."""
+        key = cell_type.lower()
+        if key not in self._type_cache:
+            ct = self.neurons["cell_type"].astype("string").str.lower()
+            if key.endswith("*"):
+                m = ct.str.startswith(key[:-1])
+            else:
+                m = ct.eq(key)
+                if "hemibrain_type" in self.neurons:
+                    m = m | self.neurons["hemibrain_type"].astype("string").str.lower().eq(key)
+            self._type_cache[key] = m.to_numpy(dtype=bool, na_value=False)
+        m = self._type_cache[key]
+        if side is not None:
+            m = m & self.neurons["side"].astype("string").eq(side).to_numpy(dtype=bool, na_value=False)
+        return np.flatnonzero(m)
+
+
+def load_flywire(data_dir) -> Connectome:
+    """The FlyWire v783 connectome from the files of Shiu et al. 2024 (neuron order of
+    ``Completeness_783.csv``; ``Connectivity_783.parquet`` pairs with their signed synapse counts,
+    duplicates added) and the FlyWire annotations (matched on the root-id column that covers the
+    most of the 783 ids)."""
+    import os
+
+    import pandas as pd
+
+    missing = [f for f in FLYWIRE_FILES if not os.path.exists(os.path.join(data_dir, f))]
+    if missing:
+        raise FileNotFoundError(f"missing {missing} in {data_dir}")
+    comp = pd.read_csv(os.path.join(data_dir, FLYWIRE_FILES[0]), index_col=0)
+    root_ids = comp.index.to_numpy(dtype=np.int64)
+    n = len(root_ids)
+    con = pd.read_parquet(os.path.join(data_dir, FLYWIRE_FILES[1]),
+                          columns=["Presynaptic_Index", "Postsynaptic_Index", "Excitatory x Connectivity"])
+    w = sp.coo_matrix((con["Excitatory x Connectivity"].to_numpy(np.float32),
+                       (con["Presynaptic_Index"].to_numpy(np.int64), con["Postsynaptic_Index"].to_numpy(np.int64))),
+                      shape=(n, n)).tocsr()
+    w.sum_duplicates()
+    w.sort_indices()
+    ann = pd.read_csv(os.path.join(data_dir, FLYWIRE_FILES[2]), sep="\t", low_memory=False)
+    id_cols = [c for c in ann.columns if c == "root_id" or c.startswith("root_")]
+    best = max(id_cols, key=lambda c: int(pd.Index(ann[c]).isin(root_ids).sum()))
+    ann = ann.drop_duplicates(best).set_index(best)
+    neurons = pd.DataFrame({"root_id": root_ids})
+    for col in _ANNOT_COLUMNS:
+        neurons[col] = ann[col].reindex(root_ids).to_numpy() if col in ann else np.nan
+    for col in ("super_class", "cell_class", "cell_type", "hemibrain_type", "side", "top_nt"):
+        neurons[col] = neurons[col].astype("string")
+    return Connectome(w, neurons, name="FlyWire v783")

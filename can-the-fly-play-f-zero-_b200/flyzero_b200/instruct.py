@@ -209,6 +209,37 @@ class BatchInstruct:
                 out += np.abs(np.asarray(targets)[:, k] - rate[:, mem].mean(1))
         return np.where(learn, out / len(self.names), 0.0)
 
+    def state(self, fly: int) -> dict:
+        """One fly's plastic weights (and learned intrinsic biases), batch.py:195-201."""
+        slot = int(np.flatnonzero(self.fly_of_slot == fly)[0])
+        st = {"pos": self.brain.plastic_pos.astype(np.int32), "data": self.brain.pw[slot].cpu().numpy(), "w0": self.w0}
+        if self.ib is not None:
+            st["bias_idx"], st["bias"] = self.dn, self.ib[slot].cpu().numpy()
+        return st
+
+    def load(self, st: dict, flies=None):
+        """Weights saved by any of the rules (matched by CSR position; positions not in the file
+        keep their connectome values) and saved intrinsic biases (batch.py:203-219)."""
+        torch = self._torch()
+        pos = self.brain.plastic_pos
+        vals = self.w0.copy()
+        where = np.searchsorted(pos, st["pos"])
+        ok = (where < len(pos)) & (pos[np.minimum(where, len(pos) - 1)] == st["pos"])
+        vals[where[ok]] = np.asarray(st["data"])[ok]
+        slots = np.arange(self.B) if flies is None else np.flatnonzero(np.isin(self.fly_of_slot, flies))
+        s = torch.as_tensor(slots, device=self.dev)
+        self.brain.pw[s] = torch.as_tensor(vals, device=self.dev)
+        if "bias" in st:
+            assert np.isin(st["bias_idx"], self.dn).all(), "saved intrinsic biases are for other neurons"
+            j = self.brain.slots(np.asarray(st["bias_idx"])).long()
+            k = torch.as_tensor(np.searchsorted(self.dn, st["bias_idx"]), device=self.dev)
+            bias = torch.as_tensor(np.asarray(st["bias"], np.float32), device=self.dev)
+            base = self.brain.bias_ext[:, j]
+            if self.ib is not None:
+                base = base - self.ib[:, k]
+                self.ib[s[:, None], k[None, :]] = bias
+            self.brain.bias_ext[s[:, None], j[None, :]] = base[s] + bias
+
     def _dn_error(self, tgt):
         """err[b][k] = target of the group of upost_k - rate[b][k] (0 for non-DN targets)."""
         torch = self._torch()

@@ -122,3 +122,32 @@ def test_batch_reward_matches_numpy_restatement(torch, scaled):
     assert np.abs(pw - gb.w0).max() > 1e-4
     same_fly = fos == 1
     np.testing.assert_array_equal(gb.pw.cpu().numpy()[same_fly][0], gb.pw.cpu().numpy()[same_fly][1])
+
+
+def test_plastic_state_round_trips_through_npz(torch, tmp_path):
+    """state() -> npz -> load() into a brain with a different plastic set: entries are matched by
+    CSR position, the others keep their connectome weights (batch.py:195-219)."""
+    from flyzero_b200.batch import BatchReward, load_state, save_state
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+
+    gb, rng, targets, fos = _batch_setup(torch)
+    br = BatchReward(gb, fly_of_slot=fos, targets=targets)
+    gb.pw += torch.as_tensor(rng.normal(0, 0.1, gb.pw.shape).astype(np.float32), device=gb.device)
+    st = br.state(1)
+    save_state(tmp_path / "fly1.npz", st)
+    back = load_state(tmp_path / "fly1.npz")
+    assert set(back) == {"pos", "data", "w0"}
+    np.testing.assert_array_equal(back["data"], gb.pw[int(np.flatnonzero(fos == 1)[0])].cpu().numpy())
+    # a second brain whose plastic set is a superset of the saved one
+    extra = np.setdiff1d(np.arange(0, gb.indices.size, 7), gb.plastic_pos)
+    pos2 = np.union1d(gb.plastic_pos, extra)
+    gb2 = BatchBrain(sp.csr_matrix((gb.data / np.float32(0.275), gb.indices, gb.indptr), shape=(gb.n, gb.n)),
+                     LIFParams(dt=0.25), batch=2, plastic_pos=pos2)
+    br2 = BatchReward(gb2, targets=targets)
+    br2.load(back)
+    got = gb2.pw.cpu().numpy()
+    k = np.searchsorted(pos2, back["pos"])
+    np.testing.assert_array_equal(got[:, k], np.tile(back["data"], (2, 1)))
+    rest = np.setdiff1d(np.arange(len(pos2)), k)
+    np.testing.assert_array_equal(got[:, rest], np.tile(gb2.w0[rest], (2, 1)))
