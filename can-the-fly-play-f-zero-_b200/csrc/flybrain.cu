@@ -16,6 +16,7 @@
 #include "plastic.cuh"
 #include "readout.cuh"
 #include "instruct.cuh"
+#include "eye.cuh"
 
 using namespace fb;
 
@@ -691,6 +692,56 @@ extern "C" int fb_backprop(const fb_brain* h, const int32_t* sel, const int32_t*
     k_backprop<<<blocks, 256, 0, (cudaStream_t)stream>>>(h->B, n_sel, sel, pre_l, post_x, x, n_x, h->pw, h->n_pl,
                                                          (float)h->params.w_syn, delta, n_delta);
     CU(cudaGetLastError());
+    return FB_OK;
+}
+
+extern "C" int64_t fb_eye_state_floats(int32_t batch, int32_t H, int32_t W, int32_t cell)
+{
+    if (batch <= 0 || cell <= 0 || H < cell || W < cell) return -1;
+    const int64_t gh = H / cell, gw = W / cell;
+    return (int64_t)batch * (8 * gh * gw + (gh + 1) * (gw + 1));
+}
+
+extern "C" int fb_motion_eye(fb_brain* h, const uint8_t* frames, int32_t H, int32_t W, const fb_eye_params* ep,
+                             float* state, uint8_t* restart, const uint8_t* flip, int32_t n_cells, const int32_t* gx,
+                             const int32_t* gy, const uint8_t* chan, const uint8_t* visible, const int32_t* slot,
+                             float* rates, void* stream)
+{
+    if (!h || !frames || !ep || !state || !restart || n_cells < 0) return fail(FB_ERR_ARG, "NULL argument");
+    if (n_cells > 0 && (!gx || !gy || !chan || !visible || !slot)) return fail(FB_ERR_ARG, "NULL argument");
+    if (ep->cell <= 0 || ep->cell > 128 || H < ep->cell || W < ep->cell || ep->shift < 1 || ep->surround < 0)
+        return fail(FB_ERR_ARG, "bad eye geometry");
+    CU(cudaSetDevice(h->device));
+    const int32_t gh = H / ep->cell, gw = W / ep->cell;
+    if (gh > 1023 || gw > 1023) return fail(FB_ERR_ARG, "eye grid wider than 1023 cells");
+    const int64_t cells = (int64_t)h->B * gh * gw;
+    EyeArgs a{};
+    a.B = h->B; a.H = H; a.W = W; a.cell = ep->cell; a.gh = gh; a.gw = gw; a.shift = ep->shift;
+    a.surround = ep->surround; a.chromatic = ep->chromatic_gain > 0.0;
+    a.a_hp = ep->a_hp; a.a_d = ep->a_d; a.gain_f = (float)ep->gain; a.max_rate = (float)ep->max_rate;
+    a.p_scale = ep->p_scale; a.transient_f = (float)ep->transient_gain; a.chromatic_f = (float)ep->chromatic_gain;
+    a.gain = ep->gain; a.sustained = ep->sustained_gain;
+    a.frames = frames; a.flip = flip; a.restart = restart;
+    a.lum = state; a.lp = a.lum + cells; a.sig = a.lp + cells; a.dly = a.sig + 2 * cells; a.col = a.dly + 2 * cells;
+    a.ii = a.col + 2 * cells;
+    a.n_cells = n_cells; a.gx = gx; a.gy = gy; a.chan = chan; a.visible = visible; a.slot = slot;
+    a.p_ext = h->p_ext; a.n_ext = (int32_t)h->n_ext; a.rates = rates;
+    cudaStream_t st = (cudaStream_t)stream;
+    int launches = 2;
+    k_eye_cells<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(a);
+    if (ep->sustained_gain != 0.0) {
+        const int t = ((std::max(gh, gw) + 1 + 31) / 32) * 32;
+        k_eye_integral<<<h->B, t, 0, st>>>(a);
+        launches++;
+    }
+    if (n_cells > 0) {
+        const int64_t work = (int64_t)h->B * n_cells;
+        k_eye_rates<<<(unsigned)((work + 255) / 256), 256, 0, st>>>(a);
+        launches++;
+    }
+    k_eye_delay<<<(unsigned)((2 * cells + 255) / 256), 256, 0, st>>>(a);
+    CU(cudaGetLastError());
+    h->launches += launches;
     return FB_OK;
 }
 

@@ -44,6 +44,12 @@ class Views(C.Structure):
                 ("bias_ext", vp), ("stop_tick", vp)]
 
 
+class EyeParams(C.Structure):
+    _fields_ = [("cell", C.c_int32), ("shift", C.c_int32), ("surround", C.c_int32), ("a_hp", C.c_float),
+                ("a_d", C.c_float), ("p_scale", C.c_float), ("gain", C.c_double), ("max_rate", C.c_double),
+                ("transient_gain", C.c_double), ("sustained_gain", C.c_double), ("chromatic_gain", C.c_double)]
+
+
 _LIB = None
 
 # every symbol include/flybrain.h declares, with its signature
@@ -65,6 +71,8 @@ SIGNATURES = {
     "fb_delta_apply": (C.c_int, [vp, vp, vp, vp, C.c_int32, vp, C.c_int32, vp, C.c_int32, vp, vp, vp, C.c_int32, vp,
                                  vp, vp]),
     "fb_backprop": (C.c_int, [vp, vp, vp, vp, C.c_int32, vp, C.c_int32, vp, C.c_int32, vp]),
+    "fb_eye_state_floats": (C.c_int64, [C.c_int32, C.c_int32, C.c_int32, C.c_int32]),
+    "fb_motion_eye": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp, vp, vp, C.c_int32, vp, vp, vp, vp, vp, vp, vp]),
     "fb_group_rates": (C.c_int, [vp, vp, vp, vp, C.c_int32, vp, C.c_float, C.c_float, vp, vp]),
     "fb_clamp": (C.c_int, [vp, vp, vp, vp, C.c_int32, vp, vp, C.c_double, C.c_double, C.c_float, C.c_float, vp, vp,
                            vp, vp, vp, vp]),

@@ -204,3 +204,33 @@ def load_flywire(data_dir) -> Connectome:
     for col in ("super_class", "cell_class", "cell_type", "hemibrain_type", "side", "top_nt"):
         neurons[col] = neurons[col].astype("string")
     return Connectome(w, neurons, name="FlyWire v783")
+
+
+# ---- biological sign corrections (flyzero/biology.py:38-55) --------------------------------------
+MODULATORY = ("dopamine", "serotonin", "octopamine")
+CORRECTIONS = ("modulatory", "kenyon_cholinergic")
+
+
+def corrected(conn: Connectome, fixes=CORRECTIONS) -> Connectome:
+    """The connectome with the reference's sign fixes (flyzero/biology.py:38-55): ``modulatory``
+    zeroes the fast weight of synapses whose presynaptic neuron's predicted transmitter is
+    dopamine, serotonin or octopamine (Kenyon cells excepted); ``kenyon_cholinergic`` makes Kenyon
+    cell outputs excitatory, inhibitory onto other Kenyon cells (with ``modulatory`` alone their
+    outputs are zeroed). Zeroed synapses are dropped from the CSR; the neuron table is shared."""
+    if not fixes:
+        return conn
+    w = conn.weights.tocoo()
+    val = w.data.copy()
+    transmitter = conn.neurons["top_nt"].fillna("").to_numpy().astype(str)
+    kenyon = conn.neurons["cell_class"].eq("Kenyon_Cell").to_numpy(dtype=bool, na_value=False)
+    from_kc = kenyon[w.row]
+    if "modulatory" in fixes:
+        val[np.isin(transmitter[w.row], MODULATORY) & ~from_kc] = 0.0
+    if "kenyon_cholinergic" in fixes:
+        size = np.abs(val[from_kc])
+        val[from_kc] = np.where(kenyon[w.col[from_kc]], -size, size)
+    elif "modulatory" in fixes:
+        val[from_kc] = 0.0
+    out = sp.csr_matrix((val, (w.row, w.col)), shape=w.shape)
+    out.eliminate_zeros()
+    return Connectome(out, conn.neurons, name=conn.name + " + corrections(" + ",".join(fixes) + ")")

@@ -197,6 +197,34 @@ int fb_delta_apply(fb_brain* brain, const int32_t* sel, const int32_t* pre_k, co
 int fb_backprop(const fb_brain* brain, const int32_t* sel, const int32_t* pre_l, const int32_t* post_x, int32_t n_sel,
                 const float* x, int32_t n_x, float* delta, int32_t n_delta, void* stream);
 
+/* Motion-vision front end (MotionEye, flyzero/vision.py:64-191) for every instance, writing the
+ * eye neurons' Poisson probabilities straight into p_ext. Parameters as MotionParams
+ * (vision.py:34-50): a_hp = float32(1 / tau_hp), a_d = float32(1 / tau_delay), p_scale =
+ * float32(dt / 1000); chromatic_gain > 0 computes the blue / green channels, sustained_gain != 0
+ * the centre-surround contrast. */
+typedef struct fb_eye_params {
+    int32_t cell, shift, surround;
+    float a_hp, a_d, p_scale;
+    double gain, max_rate, transient_gain, sustained_gain, chromatic_gain;
+} fb_eye_params;
+
+/* Floats of eye state for `batch` instances and H x W frames (-1 for a bad geometry). */
+int64_t fb_eye_state_floats(int32_t batch, int32_t H, int32_t W, int32_t cell);
+
+/* One frame per instance (MotionEye.see, vision.py:142-191). frames [device] (batch, H, W, 3)
+ * uint8; state [device] fb_eye_state_floats floats, kept between frames; restart [device] (batch)
+ * uint8: nonzero starts that instance's filters from this frame (the first frame), cleared by the
+ * call; flip [device] (batch) uint8 mirrors the frame left-right (flyzero/pool.py:44), or NULL.
+ * Per eye neuron [device]: grid column gx, row gy, channel chan (0-7 motion: polarity ON 0 / OFF 1
+ * times 4 plus screen direction right 0, left 1, down 2, up 3; 8/9 ON/OFF transient, 10/11 ON/OFF
+ * sustained, 12 blue, 13 green), visible (0 above y_min), ext slot. Writes
+ * p_ext[b][slot] = float32(max_rate * clip(gain * rate, 0, 1)) * p_scale and, unless NULL,
+ * rates [device] (batch, n_cells) in Hz. Ext slots of other neurons are left as they are. */
+int fb_motion_eye(fb_brain* brain, const uint8_t* frames, int32_t H, int32_t W, const fb_eye_params* params,
+                  float* state, uint8_t* restart, const uint8_t* flip, int32_t n_cells, const int32_t* gx,
+                  const int32_t* gy, const uint8_t* chan, const uint8_t* visible, const int32_t* slot, float* rates,
+                  void* stream);
+
 /* Choose the schedule (FB_ENGINE_*, FB_PROP_*, lanes per work item 8/16/32; 0 keeps a field). */
 int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_t lanes);
 

@@ -1,4 +1,5 @@
-"""The FlyWire v783 file loader (CPU): a tiny data directory in the three files' formats."""
+"""The FlyWire v783 file loader (CPU): a tiny data directory in the three files' formats; the
+biological sign corrections against the reference's own outputs."""
 
 import numpy as np
 import pandas as pd
@@ -25,3 +26,27 @@ def test_load_flywire_files(tmp_path):
     assert list(c.find("DNg02*")) == [2]
     assert list(c.find("MDN_x")) == [3]                       # hemibrain type
     assert list(c.neurons["root_id"]) == list(ids)
+
+
+def test_biology_corrections_match_reference(golden):
+    """``corrected`` against the reference's own biology.corrected (tests/golden/biology.npz)."""
+    import os
+    import sys
+
+    import scipy.sparse as sp
+
+    from flyzero_b200.connectome import Connectome, corrected
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_biology_golden as G
+
+    z = golden("biology.npz")
+    n = len(z["nt"])
+    w = sp.csr_matrix((z["w_data"], z["w_indices"], z["w_indptr"]), shape=(n, n))
+    df = G.neurons(z["nt"].astype(str), z["cls"].astype(str))
+    for name, fixes in G.FIXES.items():
+        c = corrected(Connectome(w, df), fixes).weights.tocsr()
+        c.sort_indices()
+        np.testing.assert_array_equal(c.indptr, z[f"{name}_indptr"], err_msg=name)
+        np.testing.assert_array_equal(c.indices, z[f"{name}_indices"], err_msg=name)
+        np.testing.assert_array_equal(c.data, z[f"{name}_data"], err_msg=name)
