@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
     ap.add_argument("--engine", default="auto", choices=["auto", "step", "persistent"])
     ap.add_argument("--lanes", type=int, default=0, help="lanes per spike work item (8/16/32; 0 = default)")
+    ap.add_argument("--component", default="brain", choices=["brain", "eye"],
+                    help="brain: the LIF engine (default); eye: the motion eye front end alone")
     return ap.parse_args()
 
 
@@ -421,16 +423,189 @@ def e2e(gb, host_rates, drive, args, fs, n_in, dev):
             "d2h_bytes_per_step": gb.B * len(drive.readout) * 4, "ms_per_step": ms / args.steps}
 
 
+EYE_METRIC = "motion-eye instance-frames/s (224x256 frames, training channels, B=64)"
+EYE_SHAPE = (224, 256)
+
+
+def eye_params():
+    from flyzero_b200.vision import MotionParams
+
+    return MotionParams(gain=10 ** 2.7, y_min=0.2, transient_gain=4.0, sustained_gain=4.0, chromatic_gain=1.0)
+
+
+def eye_oracle(lo, p):
+    from eye_oracle import EyeOracle
+
+    return EyeOracle(EYE_SHAPE, lo.gx, lo.gy, lo.chan, lo.visible, max_rate=p.max_rate, gain=p.gain, cell=p.cell,
+                     tau_hp=p.tau_hp, tau_delay=p.tau_delay, shift=p.shift, transient_gain=p.transient_gain,
+                     sustained_gain=p.sustained_gain, surround=p.surround, chromatic_gain=p.chromatic_gain)
+
+
+def eye_cpu_baseline(lo, frames, p, seconds: float) -> dict:
+    """The oracle's restatement of MotionEye.see (flyzero/vision.py:136-191), NumPy, one thread,
+    one instance, on the same frames until ~`seconds` elapse."""
+    o = eye_oracle(lo, p)
+    done, busy = 0, 0.0
+    while busy < seconds:
+        fr = frames[done % len(frames), 0]
+        t0 = time.perf_counter()
+        o.see(fr)
+        busy += time.perf_counter() - t0
+        done += 1
+    return {"value": done / busy, "unit": "instance-frames/s", "cores": 1, "kind": "port",
+            "sample": f"1 instance x {done} frames of 224x256, {busy:.1f} s, NumPy restatement of "
+                      f"flyzero/vision.py:136-191 (the reference's own operations)"}
+
+
+_EYE_CACHE: dict = {}
+
+
+def _eye_worker(job):
+    """One host process of the eye's reference arm: its own instance over its own frames; returns
+    (frames, seconds spent in see)."""
+    seed, n_frames = job
+    from flyzero_b200 import workloads as wl
+
+    if "layout" not in _EYE_CACHE:
+        from flyzero_b200 import connectome as cx
+
+        conn = cx.flywire_scale()
+        _EYE_CACHE["layout"] = wl.eye_layout(wl.grating_drive(conn.n, seed=0, exclude=conn.motor), EYE_SHAPE, 4, 0.2)
+    o = eye_oracle(_EYE_CACHE["layout"], eye_params())
+    frames = wl.game_frames(1, n_frames, EYE_SHAPE, seed=seed)
+    t0 = time.perf_counter()
+    for f in frames:
+        o.see(f[0])
+    return n_frames, time.perf_counter() - t0
+
+
+def run_eye_reference(args, world, rank):
+    """The eye's CPU path (flyzero/vision.py:136-191 restated in NumPy) on all host cores: one
+    instance per process, as the reference's pool runs one eye per worker (flyzero/pool.py:44)."""
+    import multiprocessing as mp
+
+    if rank != 0:
+        return
+    procs = len(os.sched_getaffinity(0))
+    per = 12
+    with mp.get_context("spawn").Pool(procs) as pool:
+        pool.map(_eye_worker, [(k, 1) for k in range(procs)], chunksize=1)     # build each worker's layout
+        times = []
+        for s in range(args.warmup + args.steps):
+            busy = pool.map(_eye_worker, [(1000 * s + k, per) for k in range(procs)], chunksize=1)
+            if s >= args.warmup:
+                times.append(max(t for _, t in busy))         # the processes run side by side
+    total = sum(times)
+    value = args.steps * procs * per / total
+    print(json.dumps({
+        "metric": EYE_METRIC, "value": value, "unit": "instance-frames/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8->f32", "data": "synthetic",
+        "config": {"workload": f"{per} 224x256 frames per host process per bench step, training parameters",
+                   "processes": procs},
+        "cpu_baseline": {"value": value, "unit": "instance-frames/s", "cores": procs, "kind": "port",
+                         "sample": f"{procs} instances x {per} frames per bench step; per step the slowest "
+                                   "process's time over its frames (frame generation and setup untimed)"},
+        "e2e": {"value": value, "unit": "instance-frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+        flush=True)
+
+
+def run_eye(args, world, rank, local):
+    """The motion eye alone: per bench step one frame for every instance -> fb_motion_eye -> p_ext."""
+    import torch
+
+    from flyzero_b200 import connectome as cx
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+    from flyzero_b200.vision import BatchMotionEye
+
+    dev = torch.device("cuda", local)
+    conn = cx.flywire_scale()
+    drive = wl.grating_drive(conn.n, seed=0, exclude=conn.motor)
+    B, shape, p = args.batch, EYE_SHAPE, eye_params()
+    lo = wl.eye_layout(drive, shape, p.cell, p.y_min)
+    frames = args.warmup + args.steps
+    host = wl.game_frames(B, frames, shape, seed=rank)
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=1000 + rank)
+    eye = BatchMotionEye(gb, None, shape, p, eye_layout=lo)
+    fr_dev = torch.as_tensor(host, device=dev)
+    st = torch.cuda.current_stream(dev)
+    for f in range(args.warmup):
+        eye.see(fr_dev[f])
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = gb.launches
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for k in range(args.steps):
+        eye.see(fr_dev[args.warmup + k])
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(world)
+    ms = a.elapsed_time(b)
+    launches = gb.launches - l0
+    value, max_ms = replica_value(B * args.steps, ms, world)
+    cells = (shape[0] // p.cell) * (shape[1] // p.cell)
+    n_cells = len(lo.idx)
+    # frame read + high-pass state r/w + two delay arms r/w + one p_ext write per eye neuron
+    alg = B * (shape[0] * shape[1] * 3 + cells * (8 + 16) + n_cells * 4)
+    peak, peak_kind = peaks()
+    achieved = alg / (ms / 1000.0 / args.steps) / 1e9
+    # end to end: frames from pinned host memory every step, then the eye; the rates stay on the device
+    pinned = torch.as_tensor(host).pin_memory()
+    stage = torch.empty_like(fr_dev[0])
+    eye.reset()
+    for f in range(args.warmup):
+        stage.copy_(pinned[f], non_blocking=True)
+        eye.see(stage)
+    torch.cuda.synchronize(dev)
+    a.record(st)
+    for k in range(args.steps):
+        stage.copy_(pinned[args.warmup + k], non_blocking=True)
+        eye.see(stage)
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    e2e_ms = a.elapsed_time(b)
+    out = {
+        "metric": EYE_METRIC, "value": value, "unit": "instance-frames/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8->f32", "data": "synthetic",
+        "config": {"workload": f"motion eye: {B} instances x one 224x256 RGB frame per step, cell 4 (56x64 grid), "
+                               f"{n_cells} eye neurons on 14 channels (8 motion, 6 columnar), training parameters "
+                               "(gain 10^2.7, y_min 0.2, transient 4, sustained 4, chromatic 1)",
+                   "batch": B, "eye_neurons": n_cells, "parallelism": f"replicas x{world}",
+                   "l2": "no flush: frames of all steps (%d MB) exceed the 126 MB L2" % (host.nbytes // 2 ** 20)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "model": "per instance: frame 224*256*3 B + 24 B per grid cell (high-pass and delay state "
+                              "read and written) + 4 B per eye neuron (p_ext), per call"},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": {"value": B * args.steps / (e2e_ms / 1000.0), "unit": "instance-frames/s",
+                "h2d_bytes_per_step": int(stage.numel()), "d2h_bytes_per_step": 0,
+                "note": "frames copied from pinned host memory each step; the rates stay on the device in p_ext"},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = eye_cpu_baseline(lo, host, p, min(args.cpu_seconds, 5.0))
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
-        run_reference(args, world, rank)
+        (run_eye_reference if args.component == "eye" else run_reference)(args, world, rank)
         return
     world, rank, local = dist_setup(args)
     try:
-        run_ours(args, world, rank, local)
+        (run_eye if args.component == "eye" else run_ours)(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

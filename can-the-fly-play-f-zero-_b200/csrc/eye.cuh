@@ -221,4 +221,191 @@ __global__ void k_eye_delay(const EyeArgs a)
     if (p % (2 * cells) == 0) a.restart[p / (2 * cells)] = 0;
 }
 
+// ---- the whole eye of one instance in one block ----------------------------------------------------
+// The same operations as the four kernels above, in one launch: block b reads its frame once, keeps
+// the grid (luminance, ON/OFF signals, delay arms, colour grids, integral image, float64 contrast)
+// in shared memory, writes its eye neurons' probabilities, then its new delay arms.
+
+struct EyeSmem {
+    int32_t cells, ii, chrom, sust;
+    static constexpr int32_t TAB = 766 + 256;  // pixel luminance by R+G+B, channel quotient by byte
+    __host__ __device__ size_t bytes() const
+    {
+        return (size_t)cells * 8 * sust + (size_t)cells * 4 * (5 + 2 * chrom) + (size_t)ii * 4 * sust + TAB * 4;
+    }
+};
+
+// A pixel's luminance mean(R, G, B) / 255 depends only on the integer R + G + B (the float sum of
+// three bytes is exact), and a channel value / 255 only on its byte: the tables hold those
+// quotients, computed with the same correctly rounded divisions, so the per-pixel work is a lookup.
+// VEC4: cell 4 and W a multiple of 4, so a cell row is three aligned 32-bit words.
+template <bool VEC4>
+__device__ __forceinline__ void cell_sums(const EyeArgs& a, const uint8_t* fr, bool fl, int32_t y, int32_t x,
+                                          const float* t_lum, const float* t_ch, bool chrom, float& s, float& sb,
+                                          float& sg)
+{
+    s = sb = sg = 0.0f;
+    if constexpr (VEC4) {
+        const int32_t c0 = fl ? a.W - 4 - 4 * x : 4 * x;
+#pragma unroll
+        for (int32_t yy = 0; yy < 4; yy++) {
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(fr + ((int64_t)(4 * y + yy) * a.W + c0) * 3);
+            const uint32_t w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2);
+            uint32_t ch[12];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                ch[j] = (w0 >> (8 * j)) & 255u;
+                ch[4 + j] = (w1 >> (8 * j)) & 255u;
+                ch[8 + j] = (w2 >> (8 * j)) & 255u;
+            }
+            float r = 0.0f, rb = 0.0f, rg = 0.0f;
+            auto add = [&](int p) {
+                r = __fadd_rn(r, t_lum[ch[3 * p] + ch[3 * p + 1] + ch[3 * p + 2]]);
+                if (chrom) {
+                    rb = __fadd_rn(rb, t_ch[ch[3 * p + 2]]);
+                    rg = __fadd_rn(rg, t_ch[ch[3 * p + 1]]);
+                }
+            };
+            if (fl) {                           // the mirrored frame's pixel xx is this segment's 3 - xx
+#pragma unroll
+                for (int xx = 0; xx < 4; xx++) add(3 - xx);
+            } else {
+#pragma unroll
+                for (int xx = 0; xx < 4; xx++) add(xx);
+            }
+            s = __fadd_rn(s, r);
+            sb = __fadd_rn(sb, rb);
+            sg = __fadd_rn(sg, rg);
+        }
+    } else {
+        auto px = [&](int32_t yy, int32_t xx) {
+            const int32_t c = x * a.cell + xx;
+            return fr + ((int64_t)(y * a.cell + yy) * a.W + (fl ? a.W - 1 - c : c)) * 3;
+        };
+        for (int32_t yy = 0; yy < a.cell; yy++) {
+            s = __fadd_rn(s, np_row_sum(a.cell, [&](int32_t xx) {
+                              const uint8_t* v = px(yy, xx);
+                              return t_lum[v[0] + v[1] + v[2]];
+                          }));
+            if (chrom) {
+                sb = __fadd_rn(sb, np_row_sum(a.cell, [&](int32_t xx) { return t_ch[px(yy, xx)[2]]; }));
+                sg = __fadd_rn(sg, np_row_sum(a.cell, [&](int32_t xx) { return t_ch[px(yy, xx)[1]]; }));
+            }
+        }
+    }
+}
+
+template <bool VEC4>
+__global__ void __launch_bounds__(1024) k_eye_fused(const EyeArgs a, const EyeSmem L)
+{
+    extern __shared__ __align__(16) unsigned char eye_smem[];
+    const int32_t b = blockIdx.x, cells = L.cells, W1 = a.gw + 1;
+    double* s_con = reinterpret_cast<double*>(eye_smem);
+    float* s_lum = reinterpret_cast<float*>(eye_smem + (size_t)cells * 8 * L.sust);
+    float* s_sig = s_lum + cells;                 // ON, OFF
+    float* s_dly = s_sig + 2 * cells;             // ON, OFF
+    float* s_col = s_dly + 2 * cells;             // blue, green (chromatic only)
+    float* s_ii = s_col + 2 * cells * L.chrom;    // (gh + 1) x (gw + 1) (sustained only)
+    float* t_lum = s_ii + L.ii * L.sust;          // 766 + 256 quotient tables
+    float* t_ch = t_lum + 766;
+    for (int32_t i = threadIdx.x; i < EyeSmem::TAB; i += blockDim.x) {
+        if (i < 766) t_lum[i] = __fdiv_rn(__fdiv_rn((float)i, 3.0f), 255.0f);
+        else t_ch[i - 766] = __fdiv_rn((float)(i - 766), 255.0f);
+    }
+    __syncthreads();
+    const bool restart = a.restart[b] != 0, fl = a.flip && a.flip[b];
+    const uint8_t* fr = a.frames + (int64_t)b * a.H * a.W * 3;
+    const float area = (float)(a.cell * a.cell);
+    float* lp_g = a.lp + (int64_t)b * cells;
+    float* dly_g = a.dly + (int64_t)b * 2 * cells;
+    for (int32_t q = threadIdx.x; q < cells; q += blockDim.x) {
+        const int32_t y = q / a.gw, x = q - y * a.gw;
+        float s, sb, sg;
+        cell_sums<VEC4>(a, fr, fl, y, x, t_lum, t_ch, L.chrom != 0, s, sb, sg);
+        const float lum = __fdiv_rn(s, area);
+        s_lum[q] = lum;
+        if (L.chrom) {
+            s_col[q] = __fdiv_rn(sb, area);
+            s_col[cells + q] = __fdiv_rn(sg, area);
+        }
+        float lp = restart ? lum : lp_g[q];
+        lp = __fadd_rn(lp, __fmul_rn(a.a_hp, __fsub_rn(lum, lp)));
+        lp_g[q] = lp;
+        const float hp = __fsub_rn(lum, lp);
+        s_sig[q] = fmaxf(hp, 0.0f);
+        s_sig[cells + q] = fmaxf(-hp, 0.0f);
+        s_dly[q] = restart ? 0.0f : dly_g[q];
+        s_dly[cells + q] = restart ? 0.0f : dly_g[cells + q];
+    }
+    __syncthreads();
+    if (L.sust) {
+        const int32_t t = threadIdx.x;
+        if (t <= a.gw) {                          // padded column t, down the rows
+            float c = 0.0f;
+            s_ii[t] = 0.0f;
+            for (int32_t i = 1; i <= a.gh; i++) {
+                c = __fadd_rn(c, t == 0 ? 0.0f : s_lum[(i - 1) * a.gw + t - 1]);
+                s_ii[i * W1 + t] = c;
+            }
+        }
+        __syncthreads();
+        if (t <= a.gh) {                          // row t, along the columns
+            float* r = s_ii + t * W1;
+            float c = r[0];
+            for (int32_t j = 1; j <= a.gw; j++) {
+                c = __fadd_rn(c, r[j]);
+                r[j] = c;
+            }
+        }
+        __syncthreads();
+        const int32_t rr = a.surround;
+        for (int32_t q = threadIdx.x; q < cells; q += blockDim.x) {
+            const int32_t y = q / a.gw, x = q - y * a.gw;
+            const int32_t y0 = min(max(y - rr, 0), a.gh), y1 = min(max(y + rr + 1, 0), a.gh);
+            const int32_t x0 = min(max(x - rr, 0), a.gw), x1 = min(max(x + rr + 1, 0), a.gw);
+            const float num = __fadd_rn(__fsub_rn(__fsub_rn(s_ii[y1 * W1 + x1], s_ii[y0 * W1 + x1]), s_ii[y1 * W1 + x0]),
+                                        s_ii[y0 * W1 + x0]);
+            const double sur = __ddiv_rn((double)num, (double)((int64_t)(y1 - y0) * (x1 - x0)));
+            s_con[q] = __dsub_rn((double)s_lum[q], sur);
+        }
+        __syncthreads();
+    }
+    for (int32_t k = threadIdx.x; k < a.n_cells; k += blockDim.x) {
+        const int32_t c = __ldg(a.chan + k), x = __ldg(a.gx + k), y = __ldg(a.gy + k), s = __ldg(a.slot + k);
+        if (x < 0 || x >= a.gw || y < 0 || y >= a.gh || c >= EYE_CHANNELS || s < 0 || s >= a.n_ext) continue;
+        const int32_t q = y * a.gw + x;
+        float r = 0.0f;
+        if (c < EYE_ON_TRANSIENT) {
+            const int32_t pol = c >> 2, dir = c & 3, sh = a.shift;
+            const float* sg = s_sig + pol * cells;
+            const float* dl = s_dly + pol * cells;
+            float corr = 0.0f;
+            if (dir < 2) {
+                if (x < a.gw - sh) corr = __fsub_rn(__fmul_rn(dl[q], sg[q + sh]), __fmul_rn(sg[q], dl[q + sh]));
+            } else if (y < a.gh - sh) {
+                const int32_t q1 = q + sh * a.gw;
+                corr = __fsub_rn(__fmul_rn(dl[q], sg[q1]), __fmul_rn(sg[q], dl[q1]));
+            }
+            r = (dir & 1) ? fmaxf(-corr, 0.0f) : fmaxf(corr, 0.0f);
+        } else if (c <= EYE_OFF_TRANSIENT) {
+            r = __fdiv_rn(__fmul_rn(a.transient_f, s_sig[(c - EYE_ON_TRANSIENT) * cells + q]), a.gain_f);
+        } else if (c <= EYE_OFF_SUSTAINED) {
+            if (L.sust) {
+                const double con = s_con[q];
+                const double m = c == EYE_ON_SUSTAINED ? fmax(con, 0.0) : fmax(-con, 0.0);
+                r = __double2float_rn(__ddiv_rn(__dmul_rn(a.sustained, m), a.gain));
+            }
+        } else if (L.chrom) {
+            r = __fdiv_rn(__fmul_rn(a.chromatic_f, s_col[(c - EYE_BLUE) * cells + q]), a.gain_f);
+        }
+        if (!__ldg(a.visible + k)) r = 0.0f;
+        const float rate = __fmul_rn(a.max_rate, fminf(fmaxf(__fmul_rn(a.gain_f, r), 0.0f), 1.0f));
+        if (a.rates) a.rates[(int64_t)b * a.n_cells + k] = rate;
+        a.p_ext[(int64_t)b * a.n_ext + s] = __fmul_rn(rate, a.p_scale);
+    }
+    for (int32_t q = threadIdx.x; q < 2 * cells; q += blockDim.x)
+        dly_g[q] = __fadd_rn(s_dly[q], __fmul_rn(a.a_d, __fsub_rn(s_sig[q], s_dly[q])));
+    if (threadIdx.x == 0) a.restart[b] = 0;
+}
+
 }  // namespace fb

@@ -709,7 +709,8 @@ extern "C" int fb_motion_eye(fb_brain* h, const uint8_t* frames, int32_t H, int3
 {
     if (!h || !frames || !ep || !state || !restart || n_cells < 0) return fail(FB_ERR_ARG, "NULL argument");
     if (n_cells > 0 && (!gx || !gy || !chan || !visible || !slot)) return fail(FB_ERR_ARG, "NULL argument");
-    if (ep->cell <= 0 || ep->cell > 128 || H < ep->cell || W < ep->cell || ep->shift < 1 || ep->surround < 0)
+    if (ep->cell <= 0 || ep->cell > 128 || H < ep->cell || W < ep->cell || ep->shift < 1 || ep->surround < 0 ||
+        ep->kernels < 0 || ep->kernels > 2)
         return fail(FB_ERR_ARG, "bad eye geometry");
     CU(cudaSetDevice(h->device));
     const int32_t gh = H / ep->cell, gw = W / ep->cell;
@@ -727,6 +728,22 @@ extern "C" int fb_motion_eye(fb_brain* h, const uint8_t* frames, int32_t H, int3
     a.n_cells = n_cells; a.gx = gx; a.gy = gy; a.chan = chan; a.visible = visible; a.slot = slot;
     a.p_ext = h->p_ext; a.n_ext = (int32_t)h->n_ext; a.rates = rates;
     cudaStream_t st = (cudaStream_t)stream;
+    const EyeSmem L{gh * gw, (gh + 1) * (gw + 1), a.chromatic ? 1 : 0, ep->sustained_gain != 0.0 ? 1 : 0};
+    const size_t smem = L.bytes();
+    const bool fits = smem <= 227 * 1024;
+    if (ep->kernels == 1 && !fits) return fail(FB_ERR_ARG, "eye grid too large for the one-block-per-instance kernel");
+    if (ep->kernels != 2 && fits) {
+        const bool vec4 = ep->cell == 4 && W % 4 == 0 && ((uintptr_t)frames & 3) == 0;
+        const void* fn = vec4 ? (const void*)k_eye_fused<true> : (const void*)k_eye_fused<false>;
+        CU(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        if (vec4)
+            k_eye_fused<true><<<h->B, 1024, smem, st>>>(a, L);
+        else
+            k_eye_fused<false><<<h->B, 1024, smem, st>>>(a, L);
+        CU(cudaGetLastError());
+        h->launches += 1;
+        return FB_OK;
+    }
     int launches = 2;
     k_eye_cells<<<(unsigned)((cells + 255) / 256), 256, 0, st>>>(a);
     if (ep->sustained_gain != 0.0) {

@@ -45,7 +45,8 @@ class Views(C.Structure):
 
 
 class EyeParams(C.Structure):
-    _fields_ = [("cell", C.c_int32), ("shift", C.c_int32), ("surround", C.c_int32), ("a_hp", C.c_float),
+    _fields_ = [("cell", C.c_int32), ("shift", C.c_int32), ("surround", C.c_int32), ("kernels", C.c_int32),
+                ("a_hp", C.c_float),
                 ("a_d", C.c_float), ("p_scale", C.c_float), ("gain", C.c_double), ("max_rate", C.c_double),
                 ("transient_gain", C.c_double), ("sustained_gain", C.c_double), ("chromatic_gain", C.c_double)]
 

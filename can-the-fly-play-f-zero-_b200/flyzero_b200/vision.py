@@ -3,7 +3,7 @@
 ``BatchMotionEye`` is the batched drop-in for ``flyzero.vision.MotionEye`` (flyzero/vision.py:
 64-191): one eye per instance, the same neurons in the same order (``idx``, ``px``, ``py``,
 ``side``), the same float32 filter state per instance, and ``see`` computes every instance's rates
-from a device batch of frames in four kernel launches (fb_motion_eye), writing them straight into
+from a device batch of frames in one kernel launch (fb_motion_eye), writing them straight into
 the brain's Poisson probabilities (``p_ext``) — the reference computes one eye per fly on the host
 and hands the rates to ``set_input``.
 
@@ -161,9 +161,12 @@ def _p(t):
 
 
 class BatchMotionEye:
-    """One ``MotionEye`` per instance of ``brain``; ``see`` drives the eye neurons' Poisson input."""
+    """One ``MotionEye`` per instance of ``brain``; ``see`` drives the eye neurons' Poisson input.
+    ``kernels``: "fused" runs each instance's eye in one thread block with its grid in shared
+    memory (one launch), "split" runs four grid-wide kernels, "auto" the first when it fits."""
 
-    def __init__(self, brain, conn, frame_shape, params: MotionParams | None = None, eye_layout: EyeLayout | None = None):
+    def __init__(self, brain, conn, frame_shape, params: MotionParams | None = None, eye_layout: EyeLayout | None = None,
+                 kernels: str = "auto"):
         import torch
 
         self.p = p = params or MotionParams()
@@ -186,6 +189,7 @@ class BatchMotionEye:
         self.restart = torch.ones(brain.B, dtype=torch.uint8, device=dev)
         self.rates_dev = torch.zeros((brain.B, len(lo.idx)), dtype=torch.float32, device=dev)
         self.params = _lib.EyeParams(cell=p.cell, shift=p.shift, surround=p.surround,
+                                     kernels={"auto": 0, "fused": 1, "split": 2}[kernels],
                                      a_hp=float(np.float32(1.0 / p.tau_hp)), a_d=float(np.float32(1.0 / p.tau_delay)),
                                      p_scale=float(np.float32(brain.p.dt / 1000.0)), gain=float(p.gain),
                                      max_rate=float(p.max_rate), transient_gain=float(p.transient_gain),

@@ -98,3 +98,45 @@ def high_activity_inputs(n: int, seed: int = 0, frac: float = 0.05, rate_hz: flo
     rng = np.random.default_rng(seed + 32452843)
     idx = np.sort(rng.choice(n, int(round(frac * n)), replace=False)).astype(np.int64)
     return idx, np.full(len(idx), rate_hz, np.float32)
+
+
+def game_frames(batch: int, n: int, shape=(224, 256), seed: int = 0) -> np.ndarray:
+    """Seeded synthetic game frames (n, batch, H, W, 3) uint8 in the SNES frame shape: per instance
+    a drifting grating of its own direction and speed, two moving blocks, a sky band and pixel
+    noise (stand-ins for the emulator's frames, which are not available here)."""
+    h, w = shape
+    rng = np.random.default_rng(seed + 31337)
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    out = np.empty((n, batch, h, w, 3), np.uint8)
+    ang = rng.uniform(0, 2 * np.pi, batch)
+    speed = rng.uniform(1, 6, batch)
+    blocks = rng.integers(0, [h, w], (batch, 2, 2))
+    vel = rng.integers(-5, 6, (batch, 2, 2))
+    for t in range(n):
+        for b in range(batch):
+            ph = (np.cos(ang[b]) * xx + np.sin(ang[b]) * yy + speed[b] * t) / 19.0
+            g = 0.5 + 0.5 * np.sin(2 * np.pi * ph)
+            img = np.stack([g * 180, g * 120 + 40, 255 - g * 200], -1)
+            for k in range(2):
+                y, x = (blocks[b, k] + vel[b, k] * t) % [h, w]
+                img[y:y + h // 6, x:x + w // 7] = (250, 30, 30) if k == 0 else (20, 220, 90)
+            img[: h // 8] = (90, 140, 250)
+            img += rng.integers(-12, 13, img.shape)
+            out[t, b] = np.clip(img, 0, 255).astype(np.uint8)
+    return out
+
+
+def eye_layout(drive: Drive, shape=(224, 256), cell: int = 4, y_min: float = 0.2, seed: int = 0):
+    """A motion-eye layout for the synthetic connectome (which has no cell types or positions):
+    the drive's T4/T5 stand-ins at their screen points, each on one of the 14 eye channels."""
+    from .vision import EyeLayout
+
+    h, w = shape
+    rng = np.random.default_rng(seed + 271828)
+    px = np.minimum((drive.xy[:, 0] * w).astype(np.int64), w - 1)
+    py = np.minimum((drive.xy[:, 1] * h).astype(np.int64), h - 1)
+    side = np.where(px < w // 2, "left", "right")
+    chan = rng.integers(0, 14, len(px)).astype(np.uint8)
+    gx = np.clip(px // cell, 0, w // cell - 1)
+    gy = np.clip(py // cell, 0, h // cell - 1)
+    return EyeLayout(drive.inputs, px, py, side, chan, gx, gy, ~(py < y_min * h))

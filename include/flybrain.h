@@ -201,9 +201,11 @@ int fb_backprop(const fb_brain* brain, const int32_t* sel, const int32_t* pre_l,
  * eye neurons' Poisson probabilities straight into p_ext. Parameters as MotionParams
  * (vision.py:34-50): a_hp = float32(1 / tau_hp), a_d = float32(1 / tau_delay), p_scale =
  * float32(dt / 1000); chromatic_gain > 0 computes the blue / green channels, sustained_gain != 0
- * the centre-surround contrast. */
+ * the centre-surround contrast. kernels: 0 = one block per instance when the grid fits in shared
+ * memory (else four grid-wide kernels), 1 = one block per instance (FB_ERR_ARG if it does not fit),
+ * 2 = the four grid-wide kernels. */
 typedef struct fb_eye_params {
-    int32_t cell, shift, surround;
+    int32_t cell, shift, surround, kernels;
     float a_hp, a_d, p_scale;
     double gain, max_rate, transient_gain, sustained_gain, chromatic_gain;
 } fb_eye_params;

@@ -60,5 +60,5 @@ def test_eye_params_struct_layout():
 
     from flyzero_b200._lib import EyeParams
 
-    assert C.sizeof(EyeParams) == 64
-    assert EyeParams.gain.offset == 24
+    assert C.sizeof(EyeParams) == 72
+    assert EyeParams.gain.offset == 32

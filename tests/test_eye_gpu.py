@@ -1,7 +1,8 @@
 """The motion eye on the device (fb_motion_eye) against the reference's own outputs
 (tests/golden/eye.npz) and the CPU oracle of MotionEye.see (flyzero/vision.py:136-191): every
 instance its own frames, mirrored frames (flyzero/pool.py:44), a restart in mid-sequence, the
-Poisson probabilities written into the brain's input. Bit-exact."""
+Poisson probabilities written into the brain's input; the one-block-per-instance kernel and the
+four grid-wide kernels. Bit-exact."""
 
 import numpy as np
 import pytest
@@ -40,8 +41,9 @@ def _bits(a):
     return np.asarray(a, np.float32).view(np.uint32)
 
 
+@pytest.mark.parametrize("kernels", ["fused", "split"])
 @pytest.mark.parametrize("case", E.cases(), ids=lambda c: c[1])
-def test_eye_matches_reference_and_oracle(torch, z, case):
+def test_eye_matches_reference_and_oracle(torch, z, case, kernels):
     from eye_oracle import EyeOracle
     from flyzero_b200.vision import BatchMotionEye, MotionParams, layout
 
@@ -55,7 +57,7 @@ def test_eye_matches_reference_and_oracle(torch, z, case):
     gb = _brain(int(z["n_neurons"]), B)
     bystander = int(np.setdiff1d(np.arange(gb.n), lo.idx)[0])
     gb.set_input([bystander], 42.0)
-    eye = BatchMotionEye(gb, conn, shape, p)
+    eye = BatchMotionEye(gb, conn, shape, p, kernels=kernels)
     np.testing.assert_array_equal(eye.idx, z[f"{name}_idx"])
     want = z[f"{name}_rates"]
     o_flip = EyeOracle(shape, lo.gx, lo.gy, lo.chan, lo.visible, **E.oracle_params(p))
@@ -100,6 +102,22 @@ def test_eye_drives_the_brain(torch, z):
         expect += rates.sum(1) * 0.02
     assert expect.min() > 50
     assert np.all(np.abs(total - expect) < 6 * np.sqrt(expect) + 0.1 * expect)
+
+
+def test_eye_kernels_switch_mid_sequence(torch, z):
+    """Both kernel forms keep the same state: alternating them frame by frame changes nothing."""
+    from flyzero_b200.vision import BatchMotionEye, MotionParams
+
+    k, name, shape, n, kw = E.cases()[1]
+    conn = E.connectome(z)
+    fr = E.frames(z, k, name, shape, n)
+    gb = _brain(int(z["n_neurons"]), 1)
+    eyes = [BatchMotionEye(gb, conn, shape, MotionParams(**kw), kernels=m) for m in ("fused", "split")]
+    eyes[1].state = eyes[0].state
+    eyes[1].restart = eyes[0].restart
+    for t in range(n):
+        got = eyes[t % 2].see(torch.as_tensor(fr[t:t + 1], device=gb.device)).cpu().numpy()
+        np.testing.assert_array_equal(_bits(got[0]), _bits(z[f"{name}_rates"][t]))
 
 
 def test_eye_rejects_bad_frames(torch, z):
