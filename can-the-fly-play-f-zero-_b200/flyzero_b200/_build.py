@@ -28,11 +28,26 @@ def nvcc() -> str:
     return "nvcc"
 
 
+def _digest(deps: list) -> str:
+    """SHA-256 over the sources' names and contents: what the library was built from."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for d in sorted(set(os.path.abspath(x) for x in deps)):
+        h.update(os.path.basename(d).encode())
+        with open(d, "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
 def _stale(out: str, deps: list) -> bool:
-    if not os.path.exists(out):
+    """True unless ``out`` exists and its stamp records the current sources' digest (a build that
+    read the sources before they changed leaves an old stamp, whatever the file times say)."""
+    stamp = out + ".sha256"
+    if not os.path.exists(out) or not os.path.exists(stamp):
         return True
-    t = os.path.getmtime(out)
-    return any(os.path.getmtime(d) > t for d in deps)
+    with open(stamp) as f:
+        return f.read().strip() != _digest(deps)
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
@@ -44,11 +59,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC,-O2",
            "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills", "-o", LIB + ".tmp"]
     cmd += [os.path.join(CSRC, f) for f in SOURCES]
+    digest = _digest(deps)                     # taken before nvcc reads the sources
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(LIB + ".tmp", LIB)
+    with open(LIB + ".sha256", "w") as f:
+        f.write(digest + "\n")
     return LIB
 
 
