@@ -34,6 +34,7 @@ constexpr int ZERO_PAGE = 4096;         // shared-memory zeros, the source of th
 constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulator slice
 constexpr int SPK_BUF = 1024;           // spikes of one CTA and step listed in parallel
 constexpr int IT_BUF = 384;             // work items of one CTA's epoch push staged in shared memory
+constexpr int MAX_SPECIAL = 32;         // quads with a plastic target or a bias whose inputs are staged per step
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
 constexpr int MAX_EPOCH = 4;            // steps per epoch at most (accumulator slots: twice that; 8 slots of a
                                         // 16-instance group stay in L2, which measured faster than longer epochs)
@@ -168,7 +169,7 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
 
 // Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
 struct PersistSmem {
-    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, total, words_per_map;
+    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, special, total, words_per_map;
     __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
     {
         words_per_map = (per + 4 * PT) / 32 + 1;
@@ -185,7 +186,8 @@ struct PersistSmem {
         spk = pre + 4 * MAX_EPOCH * MAX_SEG; // SPK_BUF spikes being listed
         ticks = spk + 4 * SPK_BUF;           // reset and stop ticks of up to 64 instances
         items = ticks + 2 * 64 * 8;          // IT_BUF staged work items of an epoch's push
-        total = items + 16 * IT_BUF;
+        special = items + 16 * IT_BUF;      // MAX_SPECIAL quads: biases, posts, pair, instance
+        total = special + MAX_SPECIAL * (4 * 4 + 4 * 4 + 4 + 4);
     }
 };
 
@@ -559,6 +561,10 @@ __global__ void __launch_bounds__(PT, 1)
     int64_t* s_reset = reinterpret_cast<int64_t*>(smem + lay.ticks);     // per instance of the group
     int64_t* s_stop = s_reset + 64;
     int4* s_items = reinterpret_cast<int4*>(smem + lay.items);
+    float* s_sp_bias = reinterpret_cast<float*>(smem + lay.special);           // biases (x4)
+    int32_t* s_sp_pp = reinterpret_cast<int32_t*>(s_sp_bias + 4 * MAX_SPECIAL); // plastic post index or -1 (x4)
+    int32_t* s_sp_k = s_sp_pp + 4 * MAX_SPECIAL;                               // local pair of the quad
+    int32_t* s_sp_bl = s_sp_k + MAX_SPECIAL;                                   // its instance in the group
     const Lif<float> L = N.L32;
     const int n_ref = N.n_ref;
     const int tid = threadIdx.x;
@@ -605,10 +611,32 @@ __global__ void __launch_bounds__(PT, 1)
         const int32_t k = en.x & 0x3ffff, bl = en.x >> 18;
         if (bl < G && S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + en.y] != 0.0f) sr[k] |= 0x80;
     }
+    __syncthreads();
+    // the quads with a plastic target or a biased neuron (constant during a launch), listed with their
+    // posts and biases: the neuron loop skips them and one thread per neuron advances them after it,
+    // which keeps the out-of-line call (and its local-memory traffic) off the loop's path
+    for (int32_t k = 4 * tid; k < cnt; k += 4 * PT) {
+        const uint32_t fl = *reinterpret_cast<const uint32_t*>(sr + k);
+        if ((fl & 0xc0c0c0c0u) == 0) continue;
+        const int e = atomicAdd(&s_cnt[12], 1);
+        if (e >= MAX_SPECIAL) continue;
+        const int64_t lp = lo + k;
+        const int32_t bl = (int32_t)(lp / np), i = (int32_t)(lp - (int64_t)bl * np);
+        s_sp_k[e] = k;
+        s_sp_bl[e] = bl;
+        for (int j = 0; j < 4; j++) {
+            const uint32_t f = (fl >> (8 * j)) & 0xffu;
+            const bool in = i + j < n;
+            s_sp_pp[4 * e + j] = (PLASTIC && in && (f & 0x40)) ? N.ppost_of[i + j] : -1;
+            s_sp_bias[4 * e + j] = (in && (f & 0x80)) ? S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + S.ext_idx[i + j]] : 0.0f;
+        }
+    }
     if (A.steps > 0) kicks_into<RASTER>(N, S, A, maps, 0, A.t0, A.step0, b0, G, lo, e0, e1, tid, PT, s_stop);
     __syncthreads();
 
     unsigned int barriers = 0;
+    const int n_sp = min(s_cnt[12], MAX_SPECIAL);                 // staged special quads of this CTA
+    const bool all_staged = s_cnt[12] <= MAX_SPECIAL;
     int32_t* err = S.err;
     const uint32_t acc_bytes = (uint32_t)cnt * (uint32_t)sizeof(AccT);
     const int32_t i0 = (int32_t)((lo + 4 * tid) % np), bl0 = (int32_t)((lo + 4 * tid) / np);
@@ -655,6 +683,21 @@ __global__ void __launch_bounds__(PT, 1)
                     if (tid == 0 && cnt > 0 && !staged && !ld_volatile_i32(A.abort_flag))
                         issue_slice(acc + acc_base, sacc, acc_bytes, mbar);
                     if (tid < G) s_active[tid] = t < s_stop[tid];
+                    // a staged neuron's thread: its kick of this step (the loop below overwrites the
+                    // word) and its plastic delta of this tick (complete since the last grid barrier),
+                    // whose load is consumed only after the loop
+                    uint32_t sp_kick = 0;
+                    int64_t sp_pl = 0;
+                    int64_t* sp_pl_at = nullptr;
+                    if (tid < 4 * n_sp) {
+                        const int sp = tid >> 2, j = tid & 3, blq = s_sp_bl[sp], kk = s_sp_k[sp] + j;
+                        sp_kick = (map[kk >> 5] >> (kk & 31)) & 1u;
+                        const int32_t pp = s_sp_pp[4 * sp + j];
+                        if (PLASTIC && pp >= 0 && t < s_stop[blq]) {
+                            sp_pl_at = S.pring + (pos_mod(t, N.R_pl) * N.B + (b0 + blq)) * (int64_t)N.n_ppost + pp;
+                            sp_pl = (int64_t)__ldcg(reinterpret_cast<const long long*>(sp_pl_at));
+                        }
+                    }
                     // this CTA's list segment consumed by the pushes for tick t starts empty (the
                     // step engine appends to it)
                     if (tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q, blockIdx.x) = 0;
@@ -707,9 +750,13 @@ __global__ void __launch_bounds__(PT, 1)
                                 const int32_t b = b0 + bl;
                                 int64_t* pring_row =
                                     PLASTIC ? S.pring + (pos_mod(t, N.R_pl) * N.B + b) * (int64_t)N.n_ppost : nullptr;
-                                spk4 = quad_special<AccT, PLASTIC>(sacc + k, sv + k, sg + k, sr + k, kick4, min(4, n - i),
-                                                                   pring_row, N.ppost_of + i,
-                                                                   S.bias_ext + (int64_t)b * S.n_ext, S.ext_idx + i, L, n_ref);
+                                // staged quads are advanced after the loop; the rest (a CTA with more
+                                // than MAX_SPECIAL of them) out of line here
+                                if (!all_staged)
+                                    spk4 = quad_special<AccT, PLASTIC>(sacc + k, sv + k, sg + k, sr + k, kick4,
+                                                                       min(4, n - i), pring_row, N.ppost_of + i,
+                                                                       S.bias_ext + (int64_t)b * S.n_ext, S.ext_idx + i, L,
+                                                                       n_ref);
                             }
                         }
                         // the 8 lanes of a 32-pair word OR their nibbles together; one of them stores it
@@ -720,6 +767,33 @@ __global__ void __launch_bounds__(PT, 1)
                         if ((lane & 7) == 0) map[k >> 5] = word;
                         i += 4 * U_THREADS;
                         while (i >= np) { i -= np; bl++; }
+                    }
+                    // the staged quads (plastic targets, biased neurons), one thread each, their spike
+                    // bits OR-ed into the words the loop stored
+                    if (all_staged && n_sp > 0) {
+                        u_sync();
+                        if (tid < 4 * n_sp) {            // one thread per neuron of the staged quads
+                            const int sp = tid >> 2, j = tid & 3;
+                            const int32_t kq = s_sp_k[sp], blq = s_sp_bl[sp];
+                            const int32_t iq = (int32_t)(lo + kq - (int64_t)blq * np) + j;
+                            if (iq < n && t < s_stop[blq]) {
+                                const int32_t kk = kq + j;
+                                const uint32_t f = sr[kk];
+                                float buf = acc_to_real<float>(sacc[kk], L.w_syn);
+                                if (PLASTIC && (f & 0x40)) {
+                                    buf = add_rn(buf, from_q32<float>(sp_pl));
+                                    if (sp_pl != 0) *sp_pl_at = 0;
+                                }
+                                int r = (int)(f & 0x3f);
+                                float v = sv[kk], g = sg[kk];
+                                const bool hit = lif_step<float>(v, g, r, buf, (f & 0x80) != 0, s_sp_bias[4 * sp + j],
+                                                                 sp_kick, L, n_ref, true);
+                                sv[kk] = v;
+                                sg[kk] = g;
+                                sr[kk] = (uint8_t)((f & 0xc0) | (uint32_t)r);
+                                if (hit) atomicOr(map + (kk >> 5), 1u << (kk & 31));
+                            }
+                        }
                     }
                 }
 
