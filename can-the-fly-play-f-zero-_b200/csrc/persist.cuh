@@ -295,6 +295,32 @@ __device__ __forceinline__ void kicks_into(const DevNet& N, const DevState& S, c
     }
 }
 
+// Kick threshold of an input of probability p: with u = h >> 8 < 2^24 the draw u * 2^-24 < p of
+// hash_kick holds exactly when u < ceil(p * 2^24) (the product is exact in float); 0 for p <= 0.
+__device__ __forceinline__ int32_t kick_threshold(float p)
+{
+    return p > 0.0f ? (int32_t)fminf(ceilf(__fmul_rn(p, 16777216.0f)), 16777217.0f) : 0;
+}
+
+// The Poisson kicks of a U thread's first two input pairs, held in registers for the launch as
+// {local pair | instance << 18, threshold} (the probabilities are constant during a launch): one
+// hash per pair and step, no memory read but the instance's stop tick.
+__device__ __forceinline__ void kicks_held(const DevNet& N, const DevState& S, const int2 (&kt)[2], uint32_t* map,
+                                           int64_t t, uint32_t step_no, int32_t b0, int64_t lo, const int64_t* stop)
+{
+    const uint32_t sm = step_no * 0x9e3779b9u;
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+        if (kt[u].y <= 0) continue;
+        const int32_t k = kt[u].x & 0x3ffff, bl = kt[u].x >> 18;
+        if (t >= stop[bl]) continue;
+        const int32_t b = b0 + bl;
+        const int32_t i = (int32_t)(lo + k - (int64_t)bl * N.n_pad);
+        const uint32_t h = mix32((uint32_t)((int64_t)b * N.n + i) ^ mix32(sm ^ mix32(S.seed + (uint32_t)b)));
+        if ((int32_t)(h >> 8) < kt[u].y) atomicOr(map + (k >> 5), 1u << (k & 31));
+    }
+}
+
 // Exclusive prefix of `x` over the threads tid0 = 0..stride-1 (whole warps) and the total; uses
 // `scratch` (stride / 32 entries of shared memory) and two `sync`s.
 template <typename Sync>
@@ -631,6 +657,20 @@ __global__ void __launch_bounds__(PT, 1)
             s_sp_bias[4 * e + j] = (in && (f & 0x80)) ? S.bias_ext[(int64_t)(b0 + bl) * S.n_ext + S.ext_idx[i + j]] : 0.0f;
         }
     }
+    // a U thread's first two input pairs with their kick thresholds (the rest, if a CTA has more
+    // than 2 x U_THREADS, are drawn from the table every step)
+    int2 kt[2] = {make_int2(0, 0), make_int2(0, 0)};
+    if (!RASTER && tid < U_THREADS) {
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int32_t ee = e0 + tid + u * U_THREADS;
+            if (ee < e1) {
+                const int2 en = __ldg(A.ext_tab + ee);
+                const int32_t bl = en.x >> 18;
+                if (en.y >= 0 && bl < G) kt[u] = make_int2(en.x, kick_threshold(S.p_ext[(int64_t)(b0 + bl) * S.n_ext + en.y]));
+            }
+        }
+    }
     if (A.steps > 0) kicks_into<RASTER>(N, S, A, maps, 0, A.t0, A.step0, b0, G, lo, e0, e1, tid, PT, s_stop);
     __syncthreads();
 
@@ -807,9 +847,18 @@ __global__ void __launch_bounds__(PT, 1)
                     }
                     if (tid == 0) stamp(A, s, 3);
                     // ---- the next step's kicks (they depend on nothing this step computes) --------
-                    if (s + 1 < A.steps)
-                        kicks_into<RASTER>(N, S, A, maps + ((s + 1) % 3) * wpm, s + 1, t + 1, step_no + 1u, b0, G, lo, e0,
-                                           e1, tid, U_THREADS, s_stop);
+                    if (s + 1 < A.steps) {
+                        uint32_t* mnext = maps + ((s + 1) % 3) * wpm;
+                        if (RASTER) {
+                            kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1, tid, U_THREADS,
+                                               s_stop);
+                        } else {
+                            kicks_held(N, S, kt, mnext, t + 1, step_no + 1u, b0, lo, s_stop);
+                            if (e1 - e0 > 2 * U_THREADS)
+                                kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0 + 2 * U_THREADS,
+                                                   e1, tid, U_THREADS, s_stop);
+                        }
+                    }
                     if (tid == 0) stamp(A, s, 4);
                 } else {
                     // ---- the previous step's spikes: counts, plastic rows, work items -------------
