@@ -54,8 +54,9 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
     ap.add_argument("--engine", default="auto", choices=["auto", "step", "persistent"])
     ap.add_argument("--lanes", type=int, default=0, help="lanes per spike work item (8/16/32; 0 = default)")
-    ap.add_argument("--component", default="brain", choices=["brain", "eye"],
-                    help="brain: the LIF engine (default); eye: the motion eye front end alone")
+    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet"],
+                    help="brain: the LIF engine (default); eye: the motion eye front end alone; fleet: the "
+                         "whole frame loop (frames -> eye -> brain -> readout) through the public API")
     return ap.parse_args()
 
 
@@ -596,16 +597,105 @@ def run_eye(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+FLEET_METRIC = "fleet frame loop: sim neuron-steps/s with the eye and the readout on the device (138k LIF, B=64)"
+
+
+def run_fleet(args, world, rank, local):
+    """The frame loop of flyzero/fleet.py:74-81 and batch.py:107-111 through the public API, every
+    frame: the instances' game frames from pinned host memory, the motion eye into p_ext
+    (BatchMotionEye.see), one frame of brain time (BatchBrain.run), the readout DNs' smoothed rates
+    (BatchMotor.update: device gather + EMA, the (B, 9) rates read back, the buttons on the host)."""
+    import torch
+
+    from flyzero_b200 import connectome as cx
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+    from flyzero_b200.motor import READOUT, BatchMotor
+    from flyzero_b200.vision import BatchMotionEye
+
+    dev = torch.device("cuda", local)
+    conn = cx.flywire_scale()
+    drive = wl.grating_drive(conn.n, seed=0, exclude=conn.motor)
+    pos = np.flatnonzero(np.isin(conn.weights.indices, conn.motor))
+    B, shape, p = args.batch, EYE_SHAPE, eye_params()
+    fs = wl.frame_steps(DT)
+    frames = args.warmup + args.steps
+    host = wl.game_frames(B, frames, shape, seed=rank)
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=1000 + rank, plastic_pos=pos)
+    gb.set_input(drive.tonic, 60.0)                       # the tonic DNp09 drive; the eye writes its own slots
+    eye = BatchMotionEye(gb, None, shape, p, eye_layout=wl.eye_layout(drive, shape, p.cell, p.y_min))
+    motor = BatchMotor(gb, {name: drive.readout[k:k + 1] for k, name in enumerate(READOUT)})
+    pinned = torch.as_tensor(host).pin_memory()
+    stage = torch.empty(host.shape[1:], dtype=torch.uint8, device=dev)
+    window = fs * DT
+    st = torch.cuda.current_stream(dev)
+
+    def frame(f):
+        stage.copy_(pinned[f], non_blocking=True)
+        eye.see(stage)
+        counts = gb.run(window)
+        return motor.update(counts, window)
+
+    for f in range(args.warmup):
+        frame(f)
+    gb.check()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = gb.launches
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    pressed = 0
+    for k in range(args.steps):
+        buttons = frame(args.warmup + k)
+        pressed += sum(v for bt in buttons for v in bt.values())
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    barrier(world)
+    gb.check()
+    ms = a.elapsed_time(b)
+    value, max_ms = replica_value(B * args.steps * fs * conn.n, ms, world)
+    out = {
+        "metric": FLEET_METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
+        "config": {"workload": f"fleet frame loop: {B} instances x 138,639-neuron synthetic connectome, per bench step "
+                               "one 224x256 game frame per instance -> motion eye (training channels, 12,246 eye "
+                               f"neurons) -> {fs} LIF steps at dt 0.1 ms -> readout of 9 DN groups -> buttons",
+                   "batch": B, "steps_per_frame": fs, "parallelism": f"replicas x{world}",
+                   "frames_per_s": B * args.steps / (max_ms / 1000.0), "buttons_pressed": int(pressed),
+                   "l2": "no flush: the brain's working set (state 80 MB + accumulators 71 MB + CSR 94 MB) "
+                         "exceeds the 126 MB L2"},
+        "gpu_launches": gb.launches - l0,
+        "clocks": clk,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(stage.numel()),
+                "d2h_bytes_per_step": B * len(READOUT) * 4,
+                "note": "the whole loop is end to end: frames from pinned host memory in, readout rates out"},
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
+        if args.component == "fleet":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "component": "fleet",
+                                  "unavailable": "the reference's frame loop needs its emulator pool and CuPy; "
+                                                 "see --component brain and --component eye for its two halves"}))
+            return
         (run_eye_reference if args.component == "eye" else run_reference)(args, world, rank)
         return
     world, rank, local = dist_setup(args)
     try:
-        (run_eye if args.component == "eye" else run_ours)(args, world, rank, local)
+        {"eye": run_eye, "fleet": run_fleet}.get(args.component, run_ours)(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist
