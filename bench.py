@@ -224,7 +224,7 @@ def run_reference(args, world, rank):
             times.append(dt)
     total = sum(times)
     value = args.steps * threads * steps * conn.n / total
-    print(json.dumps({
+    line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -232,7 +232,49 @@ def run_reference(args, world, rank):
                                                     "host thread, independent instances", "threads": threads},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{threads} instances x {steps} steps per bench step"},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    gpu = reference_gpu(conn, drive, idx)
+    if gpu is not None:
+        line["reference_gpu"] = gpu
+    print(json.dumps(line), flush=True)
+
+
+def reference_gpu(conn, drive, idx, frames: int = 3):
+    """The reference's own CUDA kernels (flyzero/gpu.py:26-119, built into oracle/_ref by
+    oracle/make_ref_gpu.py) with its host loop (two launches per step, gpu.py:228-254) on this
+    device, at B=1 and B=64 on the same grating workload: the reference's GPU method, for comparison."""
+    try:
+        import torch
+    except ImportError:
+        return None
+    import ref_gpu
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+
+    if not (ref_gpu.available() and torch.cuda.is_available()):
+        return None
+    fs = wl.frame_steps(DT)
+    out = {"kernels": "flyzero/gpu.py update + propagate, nvcc --use_fast_math, sm_100a, launched from Python"}
+    for B in (1, 64):
+        rb = ref_gpu.RefGpuBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=5)
+        rate = np.r_[wl.grating_rates(drive, 0.0, 0.7), np.float32(60.0)].astype(np.float32)
+        rb.set_input(idx, np.broadcast_to(rate, (B, len(idx))))
+        rb.run_steps(fs)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        spikes = 0
+        for _ in range(frames):
+            c = rb.run_steps(fs)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        spikes = int(c.sum())
+        out[f"b{B}"] = {"value": B * fs * frames * conn.n / (ms / 1000.0), "unit": UNIT, "ms_per_frame": ms / frames,
+                        "spikes_last_frame": spikes}
+        del rb
+        torch.cuda.empty_cache()
+    return out
 
 
 def spike_bytes(counts_list, rowlen_dev):
