@@ -172,6 +172,20 @@ def workload(batch: int, seed: int):
     return conn, drive, pos, work
 
 
+def cpu_model() -> str:
+    """The host CPU's model name and logical CPU count, for the CPU timings' records."""
+    name = "unknown CPU"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    name = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical CPUs, {len(os.sched_getaffinity(0))} usable"
+
+
 def cpu_baseline(conn, drive, seconds: float) -> dict:
     """The oracle's restatement of the reference kernel, one thread, on a bounded sample of the
     same workload (one instance, grating input, frames of 166 steps until ~`seconds` elapse)."""
@@ -195,7 +209,7 @@ def cpu_baseline(conn, drive, seconds: float) -> dict:
         t_ms += 166 * DT
     return {"value": steps * conn.n / busy, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"1 instance x {steps} steps ({done} frames) of the 138,639-neuron grating workload, "
-                      f"{busy:.1f} s, C port of flyzero/brain.py:32-58 (gcc -O3, AVX2)"}
+                      f"{busy:.1f} s, C port of flyzero/brain.py:32-58 (gcc -O3, AVX2)", "cpu": cpu_model()}
 
 
 def run_reference(args, world, rank):
@@ -231,7 +245,7 @@ def run_reference(args, world, rank):
         "data": "synthetic", "config": {"workload": "one 166-step frame of the 138,639-neuron grating workload per "
                                                     "host thread, independent instances", "threads": threads},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{threads} instances x {steps} steps per bench step"},
+                         "sample": f"{threads} instances x {steps} steps per bench step", "cpu": cpu_model()},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     gpu = reference_gpu(conn, drive, idx)
     if gpu is not None:
