@@ -738,6 +738,20 @@ __global__ void __launch_bounds__(PT, 1)
                             sp_pl = (int64_t)__ldcg(reinterpret_cast<const long long*>(sp_pl_at));
                         }
                     }
+                    // ---- the next step's kicks, in the shadow of the slice load: they depend on nothing
+                    //      this step computes, and their bitmap was listed and cleared in the last step
+                    if (s + 1 < A.steps) {
+                        uint32_t* mnext = maps + ((s + 1) % 3) * wpm;
+                        if (RASTER) {
+                            kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1, tid, U_THREADS,
+                                               s_stop);
+                        } else {
+                            kicks_held(N, S, kt, mnext, t + 1, step_no + 1u, b0, lo, s_stop);
+                            if (e1 - e0 > 2 * U_THREADS)
+                                kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0 + 2 * U_THREADS,
+                                                   e1, tid, U_THREADS, s_stop);
+                        }
+                    }
                     // this CTA's list segment consumed by the pushes for tick t starts empty (the
                     // step engine appends to it)
                     if (tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q, blockIdx.x) = 0;
@@ -846,19 +860,6 @@ __global__ void __launch_bounds__(PT, 1)
                         if (tid == 0 && cnt > 0) issue_slice(acc_slot<AccT>(N, S, t + 1) + acc_base, sacc, acc_bytes, mbar);
                     }
                     if (tid == 0) stamp(A, s, 3);
-                    // ---- the next step's kicks (they depend on nothing this step computes) --------
-                    if (s + 1 < A.steps) {
-                        uint32_t* mnext = maps + ((s + 1) % 3) * wpm;
-                        if (RASTER) {
-                            kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1, tid, U_THREADS,
-                                               s_stop);
-                        } else {
-                            kicks_held(N, S, kt, mnext, t + 1, step_no + 1u, b0, lo, s_stop);
-                            if (e1 - e0 > 2 * U_THREADS)
-                                kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0 + 2 * U_THREADS,
-                                                   e1, tid, U_THREADS, s_stop);
-                        }
-                    }
                     if (tid == 0) stamp(A, s, 4);
                 } else {
                     // ---- the previous step's spikes: counts, plastic rows, work items -------------
