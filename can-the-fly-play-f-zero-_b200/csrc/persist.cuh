@@ -853,7 +853,7 @@ __global__ void __launch_bounds__(PT, 1)
 
                     fence_proxy_async_shared();      // reads of the slice before the next bulk load
                     // the next step's slice, when it lies in this epoch (its arrivals are complete),
-                    // loads while the kicks are drawn
+                    // loads while this step ends
                     staged = ok && s + 1 < ep1;
                     if (staged) {
                         u_sync();
