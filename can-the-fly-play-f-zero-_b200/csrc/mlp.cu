@@ -7,7 +7,9 @@
 // backward pass), so one kernel serves them all: 128 x 64 output tiles, 8 warps of 32 x 32,
 // BF16 m16n8k16 tensor-core MMAs with FP32 accumulation, operands staged in padded shared
 // memory (conflict-free 32-bit fragment loads).
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 
@@ -307,6 +309,144 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(const uint16_t* __restri
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
+// ---------------------------------------------------------------------------------------------
+// The tcgen05 GEMM fed by the Tensor Memory Accelerator: one thread issues each K tile of A (128 rows)
+// and B (BN rows) as two 2-D TMA loads (64 bf16 = 128 bytes of K per row, 128-byte swizzle, zeros
+// outside the matrices) into a ring of TMA_STAGES shared-memory stages; one thread issues the
+// tensor-core MMAs from swizzled K-major descriptors as each stage lands and releases the stage with
+// tcgen05.commit; all four warps then read the accumulator from TMEM for the epilogue. No cluster
+// multicast anywhere. Every wait is bounded; after a timeout no result is written.
+// ---------------------------------------------------------------------------------------------
+constexpr int TMA_STAGES = 4;
+
+// shared-memory descriptor, K-major with the 128-byte swizzle: 8-row atoms of 1024 bytes (SBO), the
+// K offset inside the 128-byte row added to the start address (LBO unused: 16 bytes)
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr)
+{
+    return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(TC_THREADS) k_gemm_tma(const __grid_constant__ CUtensorMap mapA,
+                                                          const __grid_constant__ CUtensorMap mapB, int M, int N, int K,
+                                                          Epi e)
+{
+    constexpr int A_BYTES = TC_BM * 128, B_BYTES = BN * 128, STAGE = A_BYTES + B_BYTES;
+    static_assert(A_BYTES % 1024 == 0 && B_BYTES % 1024 == 0, "stages must keep 1024-byte alignment");
+    constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+    extern __shared__ uint8_t dyn[];
+    __shared__ __align__(8) uint64_t full[TMA_STAGES], empty[TMA_STAGES], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_ok, s_issued, s_used;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * TC_BM, n0 = blockIdx.x * BN;
+    const uint32_t base = (su32(dyn) + 1023u) & ~1023u;            // the swizzle needs 1024-byte atoms
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&s_tmem)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < TMA_STAGES; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&full[s])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&empty[s])) : "memory");
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(su32(&done)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_ok = 1;
+        s_issued = 0;
+        s_used = 0;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = s_tmem;
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+    const int nk = (K + 63) / 64;
+    if (tid == 0) {                                   // producer: the TMA loads
+        int kt = 0;
+        for (; kt < nk; kt++) {
+            const int s = kt % TMA_STAGES;
+            if (kt >= TMA_STAGES && !tc_wait(su32(&empty[s]), (uint32_t)((kt / TMA_STAGES - 1) & 1))) {
+                s_ok = 0;
+                break;
+            }
+            const uint32_t sa = base + s * STAGE;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(&full[s])), "r"(STAGE)
+                         : "memory");
+            tma_load_2d(sa, &mapA, kt * 64, m0, su32(&full[s]));
+            tma_load_2d(sa + A_BYTES, &mapB, kt * 64, n0, su32(&full[s]));
+        }
+        s_issued = kt;
+    } else if (tid == 32) {                           // the MMA issuer
+        int kt = 0;
+        for (; kt < nk; kt++) {
+            const int s = kt % TMA_STAGES;
+            if (!tc_wait(su32(&full[s]), (uint32_t)((kt / TMA_STAGES) & 1))) {
+                s_ok = 0;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = base + s * STAGE, sb = sa + A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {              // K = 16 per MMA: 32 bytes along the swizzled row
+                const uint64_t ad = smem_desc_sw128(sa + kk * 32), bd = smem_desc_sw128(sb + kk * 32);
+                const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             su32(&empty[s]))
+                         : "memory");
+        }
+        s_used = kt;
+        // the last commit covers every MMA issued before it
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(&done))
+                     : "memory");
+    }
+    const bool fin = tc_wait(su32(&done), 0u);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncthreads();
+    const bool ok = fin && s_ok != 0;
+    const int row = m0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t v[16];
+        const uint32_t addr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(addr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (ok) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) epilogue(e, M, N, row, n0 + c0 + j, __uint_as_float(v[j]));
+        }
+    }
+    // loads still in flight after a timeout land before the block leaves (bounded)
+    if (tid == 0)
+        for (int kt = s_used; kt < s_issued; kt++) (void)tc_wait(su32(&full[kt % TMA_STAGES]), (uint32_t)((kt / TMA_STAGES) & 1));
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
 __global__ void k_poisson(const float* z, const float* y, int M, int D, double* loss, uint16_t* dz, int ldd, uint16_t* dz_t)
 {
     __shared__ double part[8];
@@ -372,7 +512,7 @@ __global__ void k_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* ou
     }
 }
 
-int g_gemm_kind = FS_GEMM_TCGEN05;
+int g_gemm_kind = FS_GEMM_TCGEN05_TMA;
 
 int fail(const char* msg)
 {
@@ -403,6 +543,49 @@ int launch_tc(const uint16_t* A, const uint16_t* B, int M, int N, int K, int lda
     return cuda_status();
 }
 
+// A K-contiguous bf16 matrix (rows x K, row stride ld) as a TMA tensor map: boxes of 64 x box_rows
+// elements with the 128-byte swizzle. False when the driver entry point is missing or rejects it.
+bool tensor_map(CUtensorMap* map, const uint16_t* X, int rows, int K, int ld, int box_rows)
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void**)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            encode = nullptr;
+        (void)cudaGetLastError();
+    }
+    if (!encode || ((uintptr_t)X & 15) || ld % 8) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {64, (cuuint32_t)box_rows};
+    const cuuint32_t elem[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<uint16_t*>(X), dims, strides, box, elem,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// 1: launched; 0: not eligible for TMA (the caller falls back); negative: an error code
+template <int BN>
+int launch_tma(const uint16_t* A, const uint16_t* B, int M, int N, int K, int lda, int ldb, const Epi& e, cudaStream_t st)
+{
+    CUtensorMap ma, mb;
+    if (!tensor_map(&ma, A, M, K, lda, TC_BM) || !tensor_map(&mb, B, N, K, ldb, BN)) return 0;
+    constexpr int smem = TMA_STAGES * (TC_BM * 128 + BN * 128) + 1024;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_gemm_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return -cuda_status();
+        attr = true;
+    }
+    dim3 grid((N + BN - 1) / BN, (M + TC_BM - 1) / TC_BM);
+    k_gemm_tma<BN><<<grid, TC_THREADS, smem, st>>>(ma, mb, M, N, K, e);
+    const int rc = cuda_status();
+    return rc == FB_OK ? 1 : -rc;
+}
+
 unsigned blocks_for(int64_t n) { return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16)); }
 
 }  // namespace
@@ -421,7 +604,11 @@ extern "C" int fs_gemm(const uint16_t* A, const uint16_t* B, int32_t M, int32_t 
     if (epi == FS_EPI_GELU_GRAD && !zin) return fail("fs_gemm: zin needed");
     Epi e{epi, ldo, ldo_t, bias, zin, out_f32, out_bf16, out_bf16_t};
     cudaStream_t st = (cudaStream_t)stream;
-    if (g_gemm_kind == FS_GEMM_TCGEN05) {
+    if (g_gemm_kind == FS_GEMM_TCGEN05_TMA) {
+        const int rc = N <= 16 ? launch_tma<16>(A, B, M, N, K, lda, ldb, e, st) : launch_tma<64>(A, B, M, N, K, lda, ldb, e, st);
+        if (rc != 0) return rc > 0 ? FB_OK : -rc;
+    }
+    if (g_gemm_kind == FS_GEMM_TCGEN05 || g_gemm_kind == FS_GEMM_TCGEN05_TMA) {
         if (N <= 16) return launch_tc<16>(A, B, M, N, K, lda, ldb, e, st);
         return launch_tc<64>(A, B, M, N, K, lda, ldb, e, st);
     }
@@ -432,7 +619,8 @@ extern "C" int fs_gemm(const uint16_t* A, const uint16_t* B, int32_t M, int32_t 
 
 extern "C" int fs_gemm_kind(int32_t kind)
 {
-    if (kind != FS_GEMM_MMA_SYNC && kind != FS_GEMM_TCGEN05 && kind != -1) return fail("fs_gemm_kind: unknown kind");
+    if (kind != FS_GEMM_MMA_SYNC && kind != FS_GEMM_TCGEN05 && kind != FS_GEMM_TCGEN05_TMA && kind != -1)
+        return fail("fs_gemm_kind: unknown kind");
     const int old = g_gemm_kind;
     if (kind >= 0) g_gemm_kind = kind;
     return old;

@@ -26,10 +26,13 @@ extern "C" {
 #define FS_EPI_BIAS_F32 2     /* out_f32 = C + bias[j] */
 #define FS_EPI_GELU_GRAD 3    /* d = C * gelu'(zin[i][j]) -> out_bf16, transpose -> out_bf16_t */
 
-/* GEMM kinds: the BF16 m16n8k16 warp MMA, or tcgen05 (one thread issues 128 x N x 16 tensor-core
- * MMAs from shared-memory descriptors, FP32 accumulator in tensor memory); default tcgen05. */
+/* GEMM kinds: the BF16 m16n8k16 warp MMA; tcgen05 (one thread issues 128 x N x 16 tensor-core
+ * MMAs from shared-memory descriptors, FP32 accumulator in tensor memory) with operands staged by
+ * cp.async; or the same fed by TMA (2-D tensor loads with the 128-byte swizzle into a 6-stage
+ * mbarrier ring; operands whose base is not 16-byte aligned take the cp.async form). Default: TMA. */
 #define FS_GEMM_MMA_SYNC 0
 #define FS_GEMM_TCGEN05 1
+#define FS_GEMM_TCGEN05_TMA 2
 
 /* Select the kind fs_gemm uses (-1: keep); returns the previous kind. */
 int fs_gemm_kind(int32_t kind);

@@ -24,10 +24,11 @@ def _p(t):
     return None if t is None else C.c_void_p(t.data_ptr())
 
 
-@pytest.mark.parametrize("kind", [1, 0], ids=["tcgen05", "mma_sync"])
+@pytest.mark.parametrize("kind", [2, 1, 0], ids=["tcgen05_tma", "tcgen05", "mma_sync"])
 @pytest.mark.parametrize("M,N,K", [(300, 70, 200), (128, 64, 32), (37, 10, 16), (4096, 512, 1280)])
 def test_gemm_and_epilogues_match_torch_fp32(torch, M, N, K, kind):
-    """Both GEMM kinds (tcgen05 with the accumulator in tensor memory, and the warp MMA)."""
+    """Every GEMM kind: tcgen05 fed by TMA, tcgen05 fed by cp.async (accumulator in tensor memory), and
+    the warp MMA."""
     from flyzero_b200 import _lib
 
     L = _lib.load()
