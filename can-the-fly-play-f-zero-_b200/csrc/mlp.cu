@@ -4,9 +4,10 @@
 //
 // Every GEMM of the MLP's training step is written as C = A * B^T with both operands stored
 // K-contiguous (the forward pass keeps transposed copies of activations and weights for the
-// backward pass), so one kernel serves them all: 128 x 64 output tiles, 8 warps of 32 x 32,
-// BF16 m16n8k16 tensor-core MMAs with FP32 accumulation, operands staged in padded shared
-// memory (conflict-free 32-bit fragment loads).
+// backward pass), so one kernel serves them all. Three forms: k_gemm_tma (the default: tcgen05
+// MMAs, accumulator in TMEM, operands by TMA with the 128-byte swizzle), k_gemm_tc (the same with
+// cp.async staging, for operands TMA cannot describe) and k_gemm (warp-level BF16 m16n8k16 MMAs
+// on 128 x 64 tiles from padded shared memory, kept as the comparison).
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
