@@ -169,7 +169,7 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
 
 // Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
 struct PersistSmem {
-    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, special, total, words_per_map;
+    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, special, kick, total, words_per_map;
     __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
     {
         words_per_map = (per + 4 * PT) / 32 + 1;
@@ -187,7 +187,8 @@ struct PersistSmem {
         ticks = spk + 4 * SPK_BUF;           // reset and stop ticks of up to 64 instances
         items = ticks + 2 * 64 * 8;          // IT_BUF staged work items of an epoch's push
         special = items + 16 * IT_BUF;      // MAX_SPECIAL quads: biases, posts, pair, instance
-        total = special + MAX_SPECIAL * (4 * 4 + 4 * 4 + 4 + 4);
+        kick = special + MAX_SPECIAL * (4 * 4 + 4 * 4 + 4 + 4);   // kick thresholds of 2 x U_THREADS inputs
+        total = kick + 2 * U_THREADS * 4;
     }
 };
 
@@ -302,22 +303,24 @@ __device__ __forceinline__ int32_t kick_threshold(float p)
     return p > 0.0f ? (int32_t)fminf(ceilf(__fmul_rn(p, 16777216.0f)), 16777217.0f) : 0;
 }
 
-// The Poisson kicks of a U thread's first two input pairs, held in registers for the launch as
-// {local pair | instance << 18, threshold} (the probabilities are constant during a launch): one
-// hash per pair and step, no memory read but the instance's stop tick.
-__device__ __forceinline__ void kicks_held(const DevNet& N, const DevState& S, const int2 (&kt)[2], uint32_t* map,
-                                           int64_t t, uint32_t step_no, int32_t b0, int64_t lo, const int64_t* stop)
+// The Poisson kicks of a U thread's first two input pairs, held for the launch (the probabilities
+// are constant during a launch): the pair and instance {local pair | instance << 18} in registers,
+// the thresholds in shared memory; one hash per pair and step.
+__device__ __forceinline__ void kicks_held(const DevNet& N, const DevState& S, const int32_t (&kx)[2], const int32_t* s_kt,
+                                           int tid, uint32_t* map, int64_t t, uint32_t step_no, int32_t b0, int64_t lo,
+                                           const int64_t* stop)
 {
     const uint32_t sm = step_no * 0x9e3779b9u;
 #pragma unroll
     for (int u = 0; u < 2; u++) {
-        if (kt[u].y <= 0) continue;
-        const int32_t k = kt[u].x & 0x3ffff, bl = kt[u].x >> 18;
+        const int32_t thr = s_kt[u * U_THREADS + tid];
+        if (thr <= 0) continue;
+        const int32_t k = kx[u] & 0x3ffff, bl = kx[u] >> 18;
         if (t >= stop[bl]) continue;
         const int32_t b = b0 + bl;
         const int32_t i = (int32_t)(lo + k - (int64_t)bl * N.n_pad);
         const uint32_t h = mix32((uint32_t)((int64_t)b * N.n + i) ^ mix32(sm ^ mix32(S.seed + (uint32_t)b)));
-        if ((int32_t)(h >> 8) < kt[u].y) atomicOr(map + (k >> 5), 1u << (k & 31));
+        if ((int32_t)(h >> 8) < thr) atomicOr(map + (k >> 5), 1u << (k & 31));
     }
 }
 
@@ -659,16 +662,22 @@ __global__ void __launch_bounds__(PT, 1)
     }
     // a U thread's first two input pairs with their kick thresholds (the rest, if a CTA has more
     // than 2 x U_THREADS, are drawn from the table every step)
-    int2 kt[2] = {make_int2(0, 0), make_int2(0, 0)};
+    int32_t kx[2] = {0, 0};
+    int32_t* s_kt = reinterpret_cast<int32_t*>(smem + lay.kick);
     if (!RASTER && tid < U_THREADS) {
 #pragma unroll
         for (int u = 0; u < 2; u++) {
             const int32_t ee = e0 + tid + u * U_THREADS;
+            int32_t thr = 0;
             if (ee < e1) {
                 const int2 en = __ldg(A.ext_tab + ee);
                 const int32_t bl = en.x >> 18;
-                if (en.y >= 0 && bl < G) kt[u] = make_int2(en.x, kick_threshold(S.p_ext[(int64_t)(b0 + bl) * S.n_ext + en.y]));
+                if (en.y >= 0 && bl < G) {
+                    kx[u] = en.x;
+                    thr = kick_threshold(S.p_ext[(int64_t)(b0 + bl) * S.n_ext + en.y]);
+                }
             }
+            s_kt[u * U_THREADS + tid] = thr;
         }
     }
     if (A.steps > 0) kicks_into<RASTER>(N, S, A, maps, 0, A.t0, A.step0, b0, G, lo, e0, e1, tid, PT, s_stop);
@@ -746,7 +755,7 @@ __global__ void __launch_bounds__(PT, 1)
                             kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1, tid, U_THREADS,
                                                s_stop);
                         } else {
-                            kicks_held(N, S, kt, mnext, t + 1, step_no + 1u, b0, lo, s_stop);
+                            kicks_held(N, S, kx, s_kt, tid, mnext, t + 1, step_no + 1u, b0, lo, s_stop);
                             if (e1 - e0 > 2 * U_THREADS)
                                 kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0 + 2 * U_THREADS,
                                                    e1, tid, U_THREADS, s_stop);
