@@ -72,10 +72,11 @@ struct PersistArgs {
     int32_t epoch;            // K: steps between grid barriers (2K accumulator slots, 2K + 1 <= n_delay)
 };
 
-// Phase stamps (per step and CTA; SM clock cycles, compare within a CTA): 0 step start, 1 slice
-// requested, 2 slice in shared memory, 3 neurons advanced, 4 next kicks drawn, 8 listing warps
-// done with the previous step; per epoch, at its first step: 7 push warps start, 10 push warps
-// done; at its last step: 5 grid-barrier arrival, 6 grid-barrier exit (9 unused).
+// Phase stamps (per step and CTA; SM clock cycles, compare within a CTA), in step order: 0 step
+// start (the slice load issued right after), 4 the next step's kicks drawn, 1 ready to wait for the
+// slice, 2 slice in shared memory, 3 neurons advanced; 8 listing warps done with the previous
+// step; per epoch, at its first step: 7 push warps start, 10 push warps done; at its last step:
+// 5 grid-barrier arrival, 6 grid-barrier exit (9 unused).
 constexpr int TRACE_SLOTS = 11;
 
 // ---- PTX helpers: mbarrier, TMA 1-D bulk copy, proxy fences, acquire load --------------------
@@ -761,6 +762,7 @@ __global__ void __launch_bounds__(PT, 1)
                                                    e1, tid, U_THREADS, s_stop);
                         }
                     }
+                    if (tid == 0) stamp(A, s, 4);
                     // this CTA's list segment consumed by the pushes for tick t starts empty (the
                     // step engine appends to it)
                     if (tid == 64) *count_of(S, pos_mod(t - N.n_delay, N.R), q, blockIdx.x) = 0;
@@ -869,7 +871,6 @@ __global__ void __launch_bounds__(PT, 1)
                         if (tid == 0 && cnt > 0) issue_slice(acc_slot<AccT>(N, S, t + 1) + acc_base, sacc, acc_bytes, mbar);
                     }
                     if (tid == 0) stamp(A, s, 3);
-                    if (tid == 0) stamp(A, s, 4);
                 } else {
                     // ---- the previous step's spikes: counts, plastic rows, work items -------------
                     if (s >= 1)

@@ -232,10 +232,11 @@ int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_
 
 /* Phase trace of the persistent engine (diagnostics). `trace` [device] holds `capacity` int64;
  * every later fb_run whose steps * ctas * 11 fits records, per step and CTA, the SM clock at
- * these points: 0 step start, 1 accumulator slice requested, 2 slice staged, 3 neurons advanced,
- * 4 next kicks drawn, 8 listing warps done; per epoch of steps between grid barriers, at its first
- * step 7 push warps start and 10 push warps done, at its last step 5 grid-barrier arrival and
- * 6 grid-barrier exit. NULL: off. No counterpart in the reference. */
+ * these points, in step order: 0 step start (accumulator slice requested), 4 next step's kicks
+ * drawn, 1 waiting for the slice, 2 slice staged, 3 neurons advanced; 8 listing warps done; per
+ * epoch of steps between grid barriers, at its first step 7 push warps start and 10 push warps
+ * done, at its last step 5 grid-barrier arrival and 6 grid-barrier exit. NULL: off. No
+ * counterpart in the reference. */
 int fb_set_trace(fb_brain* brain, long long* trace, int64_t capacity);
 
 /* Device error flags raised since the last call (overflow, barrier timeout), then cleared.
