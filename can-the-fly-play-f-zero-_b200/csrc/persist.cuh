@@ -34,7 +34,7 @@ constexpr int ZERO_PAGE = 4096;         // shared-memory zeros, the source of th
 constexpr int LOAD_PIECE = 32768;       // bytes per bulk load of the accumulator slice
 constexpr int SPK_BUF = 1024;           // spikes of one CTA and step listed in parallel
 constexpr int IT_BUF = 384;             // work items of one CTA's epoch push staged in shared memory
-constexpr int MAX_SPECIAL = 32;         // quads with a plastic target or a bias whose inputs are staged per step
+constexpr int MAX_SPECIAL = 12;         // quads with a plastic target or a bias whose inputs are staged per step
 constexpr long long BARRIER_TIMEOUT_CYCLES = 8000000000LL;   // ~4 s at 1.9 GHz
 constexpr int MAX_EPOCH = 4;            // steps per epoch at most (accumulator slots: twice that; 8 slots of a
                                         // 16-instance group stay in L2, which measured faster than longer epochs)
@@ -187,8 +187,10 @@ struct PersistSmem {
         spk = pre + 4 * MAX_EPOCH * MAX_SEG; // SPK_BUF spikes being listed
         ticks = spk + 4 * SPK_BUF;           // reset and stop ticks of up to 64 instances
         items = ticks + 2 * 64 * 8;          // IT_BUF staged work items of an epoch's push
-        special = items + 16 * IT_BUF;      // MAX_SPECIAL quads: biases, posts, pair, instance
-        kick = special + MAX_SPECIAL * (4 * 4 + 4 * 4 + 4 + 4);   // kick thresholds of 2 x U_THREADS inputs
+        special = items + 16 * IT_BUF;      // MAX_SPECIAL quads: per step parity the accumulator values, plastic
+                                            // deltas and kicks of their neurons; biases, posts, pair, instance
+        kick = special + MAX_SPECIAL * (2 * 4 * (8 + 8 + 1) + 4 * 4 + 4 * 4 + 4 + 4);   // kick thresholds of
+                                                                                       // 2 x U_THREADS inputs
         total = kick + 2 * U_THREADS * 4;
     }
 };
@@ -591,10 +593,13 @@ __global__ void __launch_bounds__(PT, 1)
     int64_t* s_reset = reinterpret_cast<int64_t*>(smem + lay.ticks);     // per instance of the group
     int64_t* s_stop = s_reset + 64;
     int4* s_items = reinterpret_cast<int4*>(smem + lay.items);
-    float* s_sp_bias = reinterpret_cast<float*>(smem + lay.special);           // biases (x4)
+    int64_t* s_sp_acc = reinterpret_cast<int64_t*>(smem + lay.special);        // [parity][neuron] accumulator
+    int64_t* s_sp_pl = s_sp_acc + 2 * 4 * MAX_SPECIAL;                         // [parity][neuron] plastic delta
+    float* s_sp_bias = reinterpret_cast<float*>(s_sp_pl + 2 * 4 * MAX_SPECIAL); // biases (x4)
     int32_t* s_sp_pp = reinterpret_cast<int32_t*>(s_sp_bias + 4 * MAX_SPECIAL); // plastic post index or -1 (x4)
     int32_t* s_sp_k = s_sp_pp + 4 * MAX_SPECIAL;                               // local pair of the quad
     int32_t* s_sp_bl = s_sp_k + MAX_SPECIAL;                                   // its instance in the group
+    uint8_t* s_sp_kick = reinterpret_cast<uint8_t*>(s_sp_bl + MAX_SPECIAL);    // [parity][neuron] kick bit
     const Lif<float> L = N.L32;
     const int n_ref = N.n_ref;
     const int tid = threadIdx.x;
@@ -643,8 +648,10 @@ __global__ void __launch_bounds__(PT, 1)
     }
     __syncthreads();
     // the quads with a plastic target or a biased neuron (constant during a launch), listed with their
-    // posts and biases: the neuron loop skips them and one thread per neuron advances them after it,
-    // which keeps the out-of-line call (and its local-memory traffic) off the loop's path
+    // posts and biases: the neuron loop skips them; the neuron warps stage each step's inputs of their
+    // neurons (accumulator value, kick, plastic delta) and the listing warps advance them one per
+    // thread at the start of the next step, before they list that step's spikes: the out-of-line
+    // call and its local-memory traffic leave the neuron warps' path
     for (int32_t k = 4 * tid; k < cnt; k += 4 * PT) {
         const uint32_t fl = *reinterpret_cast<const uint32_t*>(sr + k);
         if ((fl & 0xc0c0c0c0u) == 0) continue;
@@ -685,8 +692,30 @@ __global__ void __launch_bounds__(PT, 1)
     __syncthreads();
 
     unsigned int barriers = 0;
-    const int n_sp = min(s_cnt[12], MAX_SPECIAL);                 // staged special quads of this CTA
     const bool all_staged = s_cnt[12] <= MAX_SPECIAL;
+    // staged special quads of this CTA (none when it has more than MAX_SPECIAL: then all of them take
+    // the out-of-line call inside the neuron loop)
+    const int n_sp = all_staged ? s_cnt[12] : 0;
+    // a staged neuron e of step s_prev (tick t_prev) from its staged inputs; its spike bit into that
+    // step's bitmap (before the step is listed)
+    auto advance_staged = [&](int32_t s_prev, int64_t t_prev, int e) {
+        const int sp = e >> 2, j = e & 3, par = s_prev & 1;
+        const int32_t kq = s_sp_k[sp], blq = s_sp_bl[sp];
+        const int32_t iq = (int32_t)(lo + kq - (int64_t)blq * np) + j;
+        if (iq >= n || t_prev >= s_stop[blq]) return;
+        const int32_t kk = kq + j;
+        const uint32_t f = sr[kk];
+        float buf = acc_to_real<float>((AccT)s_sp_acc[par * 4 * MAX_SPECIAL + e], L.w_syn);
+        if (PLASTIC && (f & 0x40)) buf = add_rn(buf, from_q32<float>(s_sp_pl[par * 4 * MAX_SPECIAL + e]));
+        int r = (int)(f & 0x3f);
+        float v = sv[kk], g = sg[kk];
+        const bool hit = lif_step<float>(v, g, r, buf, (f & 0x80) != 0, s_sp_bias[4 * sp + j],
+                                         s_sp_kick[par * 4 * MAX_SPECIAL + e], L, n_ref, true);
+        sv[kk] = v;
+        sg[kk] = g;
+        sr[kk] = (uint8_t)((f & 0xc0) | (uint32_t)r);
+        if (hit) atomicOr(maps + (s_prev % 3) * wpm + (kk >> 5), 1u << (kk & 31));
+    };
     int32_t* err = S.err;
     const uint32_t acc_bytes = (uint32_t)cnt * (uint32_t)sizeof(AccT);
     const int32_t i0 = (int32_t)((lo + 4 * tid) % np), bl0 = (int32_t)((lo + 4 * tid) / np);
@@ -735,13 +764,12 @@ __global__ void __launch_bounds__(PT, 1)
                     if (tid < G) s_active[tid] = t < s_stop[tid];
                     // a staged neuron's thread: its kick of this step (the loop below overwrites the
                     // word) and its plastic delta of this tick (complete since the last grid barrier),
-                    // whose load is consumed only after the loop
-                    uint32_t sp_kick = 0;
+                    // whose load is stored for the listing warps only after the loop
                     int64_t sp_pl = 0;
                     int64_t* sp_pl_at = nullptr;
                     if (tid < 4 * n_sp) {
                         const int sp = tid >> 2, j = tid & 3, blq = s_sp_bl[sp], kk = s_sp_k[sp] + j;
-                        sp_kick = (map[kk >> 5] >> (kk & 31)) & 1u;
+                        s_sp_kick[(s & 1) * 4 * MAX_SPECIAL + tid] = (uint8_t)((map[kk >> 5] >> (kk & 31)) & 1u);
                         const int32_t pp = s_sp_pp[4 * sp + j];
                         if (PLASTIC && pp >= 0 && t < s_stop[blq]) {
                             sp_pl_at = S.pring + (pos_mod(t, N.R_pl) * N.B + (b0 + blq)) * (int64_t)N.n_ppost + pp;
@@ -782,6 +810,8 @@ __global__ void __launch_bounds__(PT, 1)
                 // ---- advance every owned pair, four consecutive pairs per thread (a quad never straddles
                 //      two instances: rows are padded to 16); the step's kicks are read from the map and
                 //      its spikes written back into it --------------------------------------------------
+                if (ok && tid < 4 * n_sp)             // the staged neurons' accumulator values of this step
+                    s_sp_acc[(s & 1) * 4 * MAX_SPECIAL + tid] = (int64_t)sacc[s_sp_k[tid >> 2] + (tid & 3)];
                 if (ok) {
                     int32_t i = i0, bl = bl0;
                     const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
@@ -833,32 +863,10 @@ __global__ void __launch_bounds__(PT, 1)
                         i += 4 * U_THREADS;
                         while (i >= np) { i -= np; bl++; }
                     }
-                    // the staged quads (plastic targets, biased neurons), one thread each, their spike
-                    // bits OR-ed into the words the loop stored
-                    if (all_staged && n_sp > 0) {
-                        u_sync();
-                        if (tid < 4 * n_sp) {            // one thread per neuron of the staged quads
-                            const int sp = tid >> 2, j = tid & 3;
-                            const int32_t kq = s_sp_k[sp], blq = s_sp_bl[sp];
-                            const int32_t iq = (int32_t)(lo + kq - (int64_t)blq * np) + j;
-                            if (iq < n && t < s_stop[blq]) {
-                                const int32_t kk = kq + j;
-                                const uint32_t f = sr[kk];
-                                float buf = acc_to_real<float>(sacc[kk], L.w_syn);
-                                if (PLASTIC && (f & 0x40)) {
-                                    buf = add_rn(buf, from_q32<float>(sp_pl));
-                                    if (sp_pl != 0) *sp_pl_at = 0;
-                                }
-                                int r = (int)(f & 0x3f);
-                                float v = sv[kk], g = sg[kk];
-                                const bool hit = lif_step<float>(v, g, r, buf, (f & 0x80) != 0, s_sp_bias[4 * sp + j],
-                                                                 sp_kick, L, n_ref, true);
-                                sv[kk] = v;
-                                sg[kk] = g;
-                                sr[kk] = (uint8_t)((f & 0xc0) | (uint32_t)r);
-                                if (hit) atomicOr(map + (kk >> 5), 1u << (kk & 31));
-                            }
-                        }
+                    // the staged neurons' plastic deltas of this step, for the listing warps
+                    if (tid < 4 * n_sp) {
+                        s_sp_pl[(s & 1) * 4 * MAX_SPECIAL + tid] = sp_pl;
+                        if (sp_pl != 0) *sp_pl_at = 0;
                     }
                 }
 
@@ -872,7 +880,12 @@ __global__ void __launch_bounds__(PT, 1)
                     }
                     if (tid == 0) stamp(A, s, 3);
                 } else {
-                    // ---- the previous step's spikes: counts, plastic rows, work items -------------
+                    // ---- the previous step's staged neurons, then its spikes: counts, plastic rows,
+                    //      work items --------------------------------------------------------------
+                    if (s >= 1 && n_sp > 0) {
+                        if (lt < 4 * n_sp) advance_staged(s - 1, t - 1, lt);
+                        list_sync();
+                    }
                     if (s >= 1)
                         list_spikes<PLASTIC, RECORD>(N, S, A, maps + ((s - 1) % 3) * wpm, s - 1, t - 1, b0, q, lo,
                                                      used_words, s_cnt, s_scan, s_spk, lt, LIST_THREADS,
@@ -894,7 +907,12 @@ __global__ void __launch_bounds__(PT, 1)
         if (tid == 0) stamp(A, ep1 - 1, 6);
     }
     if (tid == 0) bulk_wait_all();
-    // the last step's spikes are listed before the launch ends (the next launch scatters them)
+    // the last step's staged neurons and spikes are settled before the launch ends (the next launch
+    // scatters the spikes)
+    if (last >= 0 && n_sp > 0) {
+        if (tid < 4 * n_sp) advance_staged(last, A.t0 + last, tid);
+        __syncthreads();
+    }
     if (last >= 0)
         list_spikes<PLASTIC, RECORD>(N, S, A, maps + (last % 3) * wpm, last, A.t0 + last, b0, q, lo, used_words, s_cnt,
                                      s_scan, s_spk, tid, PT, []() { __syncthreads(); });
