@@ -304,10 +304,89 @@ def spike_bytes(counts_list, rowlen_dev):
     return tot_spk, tot_edges
 
 
-# DRAM bytes (read + write) of one persistent-kernel launch of this workload (one instance group,
-# one frame), from an ncu capture; below the algorithmic bytes because the neuron state stays in
-# shared memory and most accumulator traffic stays in L2.
-K_PERSIST_DRAM_BYTES = 472_270_848 + 1_910_101_000
+def dram_traffic_record():
+    """DRAM bytes (read + write) of one persistent-kernel launch of this workload, read from the
+    committed ncu summary of that kernel (its 'traffic per launch' line names the commit and the
+    command it was measured at); None if the record is missing."""
+    import re
+
+    path = os.path.join(ROOT, "profiles", "k_persist_b64_138k.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None, None
+    m = re.search(r"traffic-per-launch-bytes:\s*([0-9_]+)\s+\(commit ([0-9a-f]+)", text)
+    if not m:
+        return None, None
+    return int(m.group(1).replace("_", "")), f"profiles/k_persist_b64_138k.md, commit {m.group(2)}"
+
+
+class Episodes:
+    """Per-instance runs of the batched workload. Instance b runs for a length drawn from
+    U{0.5, 1, 2, 3} s (5,000 - 30,000 steps), then it is reset (state, synaptic input in flight,
+    eligibility traces) and starts a new run of a fresh length, as the reference's fleet restarts a
+    fly's race. When the loop starts every instance is at a seeded random point of its first run,
+    so runs end inside any window of frames: an instance whose run ends inside a frame is frozen
+    by the engine for the rest of that frame (its run length) and restarted at the next frame."""
+
+    LENGTHS = np.array([5000, 10000, 20000, 30000], np.int64)
+
+    def __init__(self, work, seed: int, t0: int = 0):
+        self.rng = np.random.default_rng(seed)
+        first = (work.run_ms / DT).astype(np.int64)
+        self.stop = t0 + first - self.rng.integers(0, first)
+
+    def frame(self, t: int):
+        """Instances whose run ended by tick t (to reset now); draws their next run lengths."""
+        ended = np.flatnonzero(self.stop <= t)
+        self.stop[ended] = t + self.rng.choice(self.LENGTHS, len(ended))
+        return ended
+
+    def active(self, t: int, fs: int) -> np.ndarray:
+        """Steps each instance advances in the frame starting at tick t."""
+        return np.clip(self.stop - t, 0, fs)
+
+
+class FrameLoop:
+    """One bench step of the batched workload, the reference's frame (flyzero/fleet.py:74-81 with
+    the reward rule of flyzero/batch.py:482-495 / school.py:289-304): restart the instances whose
+    run ended, write the frame's rates into p_ext, run 166 steps, then the reward-modulated update
+    of every instance's plastic deltas with reward ~ N(0, 1), for the instances that ran."""
+
+    def __init__(self, gb, conn, work, rank: int, frames: int, t0: int = 0):
+        from flyzero_b200.batch import BatchReward
+
+        self.gb = gb
+        self.br = BatchReward(gb, targets=conn.motor, seed=rank)
+        self.rewards = np.random.default_rng(11 + rank).standard_normal((frames, gb.B))
+        self.ep = Episodes(work, seed=23 + rank, t0=t0)
+        self.fs = 166
+        self.t = t0
+        self.resets = 0
+        self.reset_instances = 0
+        self.public = False           # True: BatchBrain.run(ms), the reference's call
+        gb.set_stop_tick(self.ep.stop)
+
+    def __call__(self, f: int, write_rates, counts=None, events=None):
+        """One frame; ``events`` (start, end) CUDA events are recorded around the engine's run."""
+        gb = self.gb
+        ended = self.ep.frame(self.t)
+        if len(ended):
+            gb.reset(ended)
+            self.br.reset(ended)
+            gb.set_stop_tick(self.ep.stop)
+            self.resets += 1
+            self.reset_instances += len(ended)
+        act = self.ep.active(self.t, self.fs)
+        write_rates(f)
+        if events:
+            events[0].record()
+        c = gb.run(self.fs * DT) if self.public else gb.run_steps(self.fs, counts=counts)
+        if events:
+            events[1].record()
+        self.br.step(c, self.rewards[f], act > 0, self.fs * DT)
+        self.t += self.fs
+        return c, int(act.sum())
 
 
 def run_ours(args, world, rank, local):
@@ -321,6 +400,7 @@ def run_ours(args, world, rank, local):
     conn, drive, pos, work = workload(args.batch, seed=rank)
     B, n = args.batch, conn.n
     fs = wl.frame_steps(DT)
+    assert fs == 166
     frames = args.warmup + args.steps
     gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=1000 + rank, plastic_pos=pos)
     gb.set_schedule(args.engine, lanes=args.lanes)
@@ -329,10 +409,6 @@ def run_ours(args, world, rank, local):
     assert np.array_equal(np.sort(j), np.arange(len(idx_in))), "inputs own the first ext slots"
     inv = np.empty_like(j)
     inv[j] = np.arange(len(j))
-    # per-instance plastic deltas (the reward rule's state after some learning)
-    dw = np.random.default_rng(7 + rank).standard_normal((B, len(pos))).astype(np.float32) * np.float32(0.05)
-    gb.pw += torch.as_tensor(dw, device=dev)
-    gb.set_run_length((work.run_ms / DT).astype(np.int64))
     # every frame's rates, resident on the device, already in ext-slot order and scaled to p
     t_ms = 0.0
     host_rates = np.empty((frames, B, len(idx_in)), np.float32)
@@ -345,63 +421,76 @@ def run_ours(args, world, rank, local):
     rowlen = torch.as_tensor(np.diff(conn.weights.indptr), device=dev)
     n_in = len(idx_in)
     st = torch.cuda.current_stream(dev)
+    loop = FrameLoop(gb, conn, work, rank, frames)
 
-    def frame(f):
+    def rates(f):
         gb.p_ext[:, :n_in].copy_(p_dev[f])
-        gb.run_steps(fs, counts=counts[f])
 
     for f in range(args.warmup):
-        frame(f)
+        loop(f, rates, counts[f])
     gb.check()
     torch.cuda.synchronize(dev)
     barrier(world)
     torch.cuda.synchronize(dev)
     launches0 = gb.launches
+    resets0, reset_inst0 = loop.resets, loop.reset_instances
     clocks = Clocks(local)
     clocks.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     e_all0, e_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    active = 0
+    l_run = 0
     e_all0.record(st)
     for k in range(args.steps):
         f = args.warmup + k
-        gb.p_ext[:, :n_in].copy_(p_dev[f])
-        ev[k][0].record(st)
-        gb.run_steps(fs, counts=counts[f])
-        ev[k][1].record(st)
+        l0 = gb.launches
+        _, a = loop(f, rates, counts[f], events=ev[k])     # events around the run's launches
+        l_run += gb.launches - l0
+        active += a
     e_all1.record(st)
     torch.cuda.synchronize(dev)
     clk = clocks.stop()
     barrier(world)
     gb.check()
     elapsed_ms = e_all0.elapsed_time(e_all1)
-    kernel_ms = sum(a.elapsed_time(b) for a, b in ev)
-    launches = gb.launches - launches0 + args.steps          # + one p_ext copy kernel per frame
-    t0 = args.warmup * fs
-    stop = (work.run_ms / DT).astype(np.int64)
-    active = int(sum(np.clip(stop - (t0 + k * fs), 0, fs).sum() for k in range(args.steps)))
+    run_ms = sum(a.elapsed_time(b) for a, b in ev)     # the engine's runs alone (persistent launches)
+    # per frame: the engine's launches (runs, resets, reward steps) + one p_ext copy kernel
+    launches = gb.launches - launches0 + args.steps
     neuron_steps = active * n
     value, max_ms = replica_value(neuron_steps, elapsed_ms, world)
     spk, edges = spike_bytes(counts[args.warmup:], rowlen)
     alg_bytes = BYTES_PER_NEURON_STEP * neuron_steps + BYTES_PER_SPIKE * spk + BYTES_PER_EDGE * edges
     info = gb.info()
-    n_kernel_launches = max(1, launches - args.steps)
     peak, peak_kind = peaks()
-    achieved = (alg_bytes / n_kernel_launches) / ((kernel_ms / 1000.0) / n_kernel_launches) / 1e9
+    n_kern = max(1, l_run)      # the engine's launches inside the runs: one per instance group per frame
+    achieved = (alg_bytes / n_kern) / (run_ms / 1000.0 / n_kern) / 1e9
+    traffic, traffic_src = dram_traffic_record()
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+i32", "data": "synthetic",
         "config": {"workload": "batched: 64 instances x 138,639-neuron synthetic connectome, 1 frame = 166 steps "
-                               "at dt 0.1 ms per bench step, grating + tonic Poisson input, 7,300 plastic synapses",
+                               "at dt 0.1 ms per bench step, grating + tonic Poisson input, 7,300 plastic synapses "
+                               "onto 8 motor neurons updated every frame by the reward rule (reward ~ N(0,1))",
                    "neurons": n, "connections": int(conn.nnz), "synapses": conn.synapses(), "batch": B,
                    "steps_per_frame": fs, "active_instance_steps": active, "parallelism": f"replicas x{world}",
                    "engine": "persistent" if info.group else "step", "group": int(info.group),
+                   "in_timed_loop": "per frame: restart of ended runs (fb_reset of those instances + stop ticks), "
+                                    "p_ext write, run(166 steps) with per-instance run-length masking, "
+                                    "BatchReward.step on the frame's counts",
+                   "run_lengths": "U{0.5,1,2,3} s per run, each instance starting at a seeded random point of its "
+                                  "first run; ended runs are reset and restarted at the next frame",
+                   "runs_restarted_in_timed_loop": loop.reset_instances - reset_inst0,
+                   "frames_with_restarts": loop.resets - resets0,
                    "l2": "no flush: working set (state 80 MB + accumulators 71 MB + CSR 94 MB) exceeds the 126 MB L2",
                    "spikes": spk, "mean_rate_hz": spk / max(1, active) / (DT / 1000.0) / n * 1.0},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": K_PERSIST_DRAM_BYTES if info.group else None, "peak_kind": peak_kind,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_persist launch "
-                                       "of this workload (bench.py --steps 2 --warmup 3 --no-cpu --no-extras)",
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "traffic": traffic if info.group else None, "peak_kind": peak_kind,
+                     "traffic_source": traffic_src,
+                     "kernel_ms_per_launch": run_ms / n_kern, "kernel_launches": n_kern,
+                     "kernel_timing": "CUDA events on the launching stream around each frame's run (its "
+                                      "persistent launches) inside the timed loop",
                      "model": "26 B per instance-neuron-step + 16 B per spike + 14 B per edge pushed, per launch of the "
                               "persistent kernel (one per instance group per frame)"},
         "gpu_launches": launches,
@@ -409,7 +498,7 @@ def run_ours(args, world, rank, local):
     }
     if not args.no_extras:
         out["plain_b1"] = plain_b1(conn, drive, dev)
-        out["e2e"] = e2e(gb, host_rates, drive, args, fs, n_in, dev)
+        out["e2e"] = e2e(conn, work, drive, host_rates, args, fs, n_in, inv, dev, rank, pos)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(conn, drive, args.cpu_seconds)
     if rank == 0:
@@ -443,41 +532,58 @@ def plain_b1(conn, drive, dev, frames: int = 6):
             "ms_per_frame": ms / frames, "spikes_last_frame": int(c.sum())}
 
 
-def e2e(gb, host_rates, drive, args, fs, n_in, dev):
-    """End to end through the public API with host buffers: per frame, H2D of the frame's rates from
-    pinned memory, the p_ext write (Fleet.think, flyzero/fleet.py:76-77), run(16.64 ms) and a D2H
-    read of the readout DNs' counts (BatchMotor.update reads DN counts, flyzero/batch.py:109)."""
+def e2e(conn, work, drive, host_rates, args, fs, n_in, inv, dev, rank, pos):
+    """End to end through the public API with host buffers, on a fresh engine: per frame, the
+    restart of ended runs (BatchBrain.reset of those instances + stop ticks), H2D of the frame's
+    rates from pinned memory and the p_ext write (Fleet.think, flyzero/fleet.py:76-77),
+    BatchBrain.run(16.64 ms), BatchReward.step with the frame's rewards (batch.py:482-495) and a
+    D2H read of the readout DNs' counts (BatchMotor.update reads DN counts, flyzero/batch.py:109)."""
     import torch
 
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+
+    B = args.batch
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=B, seed=2000 + rank, plastic_pos=pos)
+    gb.set_schedule(args.engine, lanes=args.lanes)
+    gb.slots(np.r_[drive.inputs, drive.tonic])
+    frames = args.warmup + args.steps
     pinned = torch.as_tensor(host_rates).pin_memory()
     readout = torch.as_tensor(drive.readout, device=dev)
-    out_h = torch.empty((args.steps, gb.B, len(drive.readout)), dtype=torch.int32).pin_memory()
-    stage = torch.empty((gb.B, n_in), dtype=torch.float32, device=dev)
+    out_h = torch.empty((args.steps, B, len(drive.readout)), dtype=torch.int32).pin_memory()
+    stage = torch.empty((B, n_in), dtype=torch.float32, device=dev)
     scale = torch.tensor(np.float32(DT / 1000.0), device=dev)
     st = torch.cuda.current_stream(dev)
-    gb.reset()
-    for f in range(args.warmup):              # the same calls as a timed frame, readout included
+    loop = FrameLoop(gb, conn, work, rank, frames)
+    loop.public = True
+
+    def rates(f):
         stage.copy_(pinned[f], non_blocking=True)
         torch.mul(stage, scale, out=gb.p_ext[:, :n_in])
-        c = gb.run(fs * DT)
+
+    for f in range(args.warmup):              # the same calls as a timed frame, readout included
+        c, _ = loop(f, rates)
         out_h[0].copy_(c.index_select(1, readout), non_blocking=True)
     torch.cuda.synchronize(dev)
+    r0 = loop.resets
+    active = 0
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(st)
     for k in range(args.steps):
-        f = args.warmup + k
-        stage.copy_(pinned[f], non_blocking=True)
-        torch.mul(stage, scale, out=gb.p_ext[:, :n_in])
-        c = gb.run(fs * DT)
+        c, act = loop(args.warmup + k, rates)
         out_h[k].copy_(c.index_select(1, readout), non_blocking=True)
+        active += act
     b.record(st)
     torch.cuda.synchronize(dev)
+    gb.check()
     ms = a.elapsed_time(b)
-    t0 = args.warmup * fs
-    stop = np.asarray(gb.stop_tick.cpu().numpy())
-    active = int(sum(np.clip(stop - (t0 + k * fs), 0, fs).sum() for k in range(args.steps)))
-    return {"value": active * gb.n / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": gb.B * n_in * 4,
-            "d2h_bytes_per_step": gb.B * len(drive.readout) * 4, "ms_per_step": ms / args.steps}
+    restarts = loop.resets - r0
+    # rates + reward coefficients (f64) and fly weights (f32) every frame; stop ticks (i64) and the
+    # reset list (one byte per instance) on frames that restart runs
+    h2d = B * n_in * 4 + B * (8 + 4) + (B * (8 + 1) * restarts) // max(1, args.steps)
+    return {"value": active * gb.n / (ms / 1000.0), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": B * len(drive.readout) * 4, "ms_per_step": ms / args.steps,
+            "frames_with_restarts": restarts}
 
 
 EYE_METRIC = "motion-eye instance-frames/s (224x256 frames, training channels, B=64)"

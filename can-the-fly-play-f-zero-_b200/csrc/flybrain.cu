@@ -181,6 +181,13 @@ struct fb_brain {
     int64_t* reset_tick = nullptr;
     int64_t* stop_tick = nullptr;
     uint8_t* fly_mask = nullptr;
+    // pinned staging of fb_reset's instance masks: a ring of buffers, each reused only after the
+    // copy that read it completed (its event), so a partial reset never blocks on the stream
+    static constexpr int MASK_RING = 4;
+    uint8_t* mask_h[MASK_RING] = {nullptr};
+    cudaEvent_t mask_ev[MASK_RING] = {nullptr};
+    bool mask_used[MASK_RING] = {false};
+    int mask_at = 0;
     long long* trace = nullptr;   // caller's phase-trace buffer (fb_set_trace) or nullptr
     int64_t trace_cap = 0;
     int32_t* err_h = nullptr;   // host-mapped flags
@@ -234,6 +241,10 @@ int free_all(fb_brain* h)
         if (p) cudaFree(p);
     for (void* p : h->graveyard) cudaFree(p);
     if (h->err_h) cudaFreeHost(h->err_h);
+    for (int k = 0; k < fb_brain::MASK_RING; k++) {
+        if (h->mask_ev[k]) cudaEventDestroy(h->mask_ev[k]);
+        if (h->mask_h[k]) cudaFreeHost(h->mask_h[k]);
+    }
     return FB_OK;
 }
 
@@ -537,13 +548,20 @@ extern "C" int fb_reset(fb_brain* h, const int32_t* flies, int32_t n_flies, void
     const bool all = (flies == nullptr || n_flies < 0);
     const uint8_t* mask = nullptr;
     if (!all) {
-        std::vector<uint8_t> m(h->B, 0);
-        for (int32_t k = 0; k < n_flies; k++) {
+        for (int32_t k = 0; k < n_flies; k++)
             if (flies[k] < 0 || flies[k] >= h->B) return fail(FB_ERR_ARG, "fly %d out of range", flies[k]);
-            m[flies[k]] = 1;
+        const int r = h->mask_at;
+        h->mask_at = (r + 1) % fb_brain::MASK_RING;
+        if (!h->mask_h[r]) {
+            CU(cudaHostAlloc((void**)&h->mask_h[r], (size_t)h->B, cudaHostAllocDefault));
+            CU(cudaEventCreateWithFlags(&h->mask_ev[r], cudaEventDisableTiming));
         }
-        CU(cudaMemcpyAsync(h->fly_mask, m.data(), h->B, cudaMemcpyHostToDevice, st));
-        CU(cudaStreamSynchronize(st));   // the host vector dies at return
+        if (h->mask_used[r]) CU(cudaEventSynchronize(h->mask_ev[r]));   // its last copy has been read
+        std::memset(h->mask_h[r], 0, (size_t)h->B);
+        for (int32_t k = 0; k < n_flies; k++) h->mask_h[r][flies[k]] = 1;
+        CU(cudaMemcpyAsync(h->fly_mask, h->mask_h[r], h->B, cudaMemcpyHostToDevice, st));
+        CU(cudaEventRecord(h->mask_ev[r], st));
+        h->mask_used[r] = true;
         mask = h->fly_mask;
     }
     const int64_t total = (int64_t)h->B * h->n;

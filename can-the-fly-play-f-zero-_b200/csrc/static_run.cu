@@ -66,8 +66,10 @@ __global__ void __launch_bounds__(256) k_static_step(const StaticArgs a, int64_t
     L.v_rest = a.v_rest;
     L.v_th = a.v_th;
     L.v_reset = a.v_reset;
-    int64_t* in_slot = ring + (t % a.R) * a.n;
-    int64_t* out_slot = ring + ((t + a.n_delay) % a.R) * a.n;
+    // non-negative slots even for a negative tick (the host rejects t0 < 0 as well)
+    const int64_t si = ((t % a.R) + a.R) % a.R, so = (((t + a.n_delay) % a.R) + a.R) % a.R;
+    int64_t* in_slot = ring + si * a.n;
+    int64_t* out_slot = ring + so * a.n;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < a.n; base += stride) {
         const int64_t i = base + threadIdx.x;
@@ -118,7 +120,9 @@ int static_fail(int code, const char* fmt, ...)
     return code;
 }
 
-// Device address of the scratch for the current device, looked up once per device.
+// Device address of the scratch for the current device, looked up once per device. A device reset
+// (cudaDeviceReset, or any teardown of the primary context) reloads the module, possibly at another
+// address, so the cached address is only valid for the context it was looked up in.
 int static_scratch(int64_t** out)
 {
     int dev = 0;
@@ -151,16 +155,25 @@ extern "C" int fb_run_static(const fb_params* p, int64_t n, const int64_t* indpt
         return static_fail(FB_ERR_ARG, "fb_run_static: NULL pointer or bad size");
     if (ext_idx && (!p_ext || !bias_ext))
         return static_fail(FB_ERR_ARG, "fb_run_static: ext_idx needs p_ext and bias_ext");
-    if (p->dt <= 0 || p->tau_m <= 0 || p->tau_syn <= 0)
-        return static_fail(FB_ERR_ARG, "fb_run_static: dt, tau_m, tau_syn must be > 0");
-    const int64_t nd = std::max<int64_t>(1, (int64_t)std::nearbyint(p->delay / p->dt));
-    const int64_t nr = (int64_t)std::nearbyint(p->t_ref / p->dt);
+    if (!(p->dt > 0) || !(p->tau_m > 0) || !(p->tau_syn > 0) || !std::isfinite(p->dt))
+        return static_fail(FB_ERR_ARG, "fb_run_static: dt, tau_m, tau_syn must be finite and > 0");
+    // ticks index the ring as t mod (n_delay + 1): they must stay non-negative for the whole call
+    if (t0 < 0 || t0 > INT64_MAX - (int64_t)steps)
+        return static_fail(FB_ERR_ARG, "fb_run_static: t0=%lld must be >= 0 and t0 + steps must not overflow",
+                           (long long)t0);
+    // delay/dt and t_ref/dt are rounded to step counts; reject values whose rounding is not a small integer
+    const double dq = p->delay / p->dt, rq = p->t_ref / p->dt;
+    if (!std::isfinite(dq) || !std::isfinite(rq) || std::fabs(dq) > 1e6 || rq > 1e6 || rq < -0.5)
+        return static_fail(FB_ERR_ARG, "fb_run_static: delay/dt must be finite with |delay/dt| <= 1e6, t_ref/dt finite in [0, 1e6]");
+    const int64_t nd = std::max<int64_t>(1, (int64_t)std::nearbyint(dq));
+    const int64_t nr = (int64_t)std::nearbyint(rq);
     if (nr < 0 || nr > 127) return static_fail(FB_ERR_ARG, "fb_run_static: n_ref=%lld must fit int8", (long long)nr);
-    if (n > (int64_t)INT32_MAX - 1 || n * (nd + 1) > (int64_t)FB_STATIC_RING_ENTRIES)
+    // division, not n * (nd + 1): the product could overflow for huge n
+    if (n > (int64_t)INT32_MAX - 1 || nd + 1 > (int64_t)FB_STATIC_RING_ENTRIES / n)
         return static_fail(FB_ERR_ARG,
-                           "fb_run_static: n * (n_delay + 1) = %lld exceeds the static ring of %lld entries "
+                           "fb_run_static: n * (n_delay + 1) = %lld * %lld exceeds the static ring of %lld entries "
                            "(use fb_create/fb_run for larger networks)",
-                           (long long)(n * (nd + 1)), (long long)FB_STATIC_RING_ENTRIES);
+                           (long long)n, (long long)(nd + 1), (long long)FB_STATIC_RING_ENTRIES);
     int64_t* ring = nullptr;
     int rc = static_scratch(&ring);
     if (rc) return rc;

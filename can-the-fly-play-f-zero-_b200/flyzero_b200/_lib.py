@@ -159,3 +159,27 @@ def device_tensor(address: int, shape, dtype: str, device, owner):
     if int(np.prod(shape)) == 0 or not address:
         return torch.empty(tuple(shape), dtype=getattr(torch, dtype), device=device)
     return torch.as_tensor(_DeviceArray(address, shape, _TYPESTR[dtype], owner), device=device)
+
+
+class HostStage:
+    """Small per-call host arrays copied to the device without blocking the host: a ring of pinned
+    buffers, each refilled only after the stream has consumed the copy that last read it (an event
+    per buffer). ``put(dst, values)`` enqueues dst <- values on the current stream."""
+
+    def __init__(self, n: int, dtype, slots: int = 4):
+        import torch
+
+        self._ring = [[torch.empty(n, dtype=dtype).pin_memory(), None] for _ in range(slots)]
+        self._at = 0
+
+    def put(self, dst, values):
+        import torch
+
+        buf = self._ring[self._at]
+        self._at = (self._at + 1) % len(self._ring)
+        if buf[1] is not None:
+            buf[1].synchronize()
+        buf[0].numpy()[:] = values
+        dst.copy_(buf[0], non_blocking=True)
+        buf[1] = torch.cuda.Event()
+        buf[1].record(torch.cuda.current_stream(dst.device))

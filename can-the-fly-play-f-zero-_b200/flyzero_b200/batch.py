@@ -4,8 +4,8 @@ the plastic bookkeeping of ``flyzero.batch`` (flyzero/batch.py:141-223, 454-495)
 Several slots (instances running different races) can belong to one fly (``fly_of_slot``): their
 weight changes are averaged over the fly's learning slots and applied to every slot of the fly,
 the sequential rule with a larger batch. ``BatchReward.step`` runs as one fused CUDA kernel pair
-(fb_reward_step); ``_Plastic.apply`` keeps the reference's generic form (any ``dw``) in torch for
-other rules.
+(fb_reward_step); ``_Plastic.apply`` takes any ``dw`` through the engine's fused per-fly delta
+kernel (fb_delta_apply).
 
 Arithmetic follows NumPy's promotion rules, as the CPU rule (flyzero/learning.py) computes them:
 float64 eligibility traces, float32 running means, float32 weights.
@@ -52,7 +52,14 @@ def _ptr(t):
 
 
 class _Plastic:
-    """Shared bookkeeping: the brain's plastic synapses, their caps and slot -> fly grouping."""
+    """Per-slot plastic weights of a ``BatchBrain`` grouped into flies, kept on the device.
+
+    The engine stores slot b's weights as row b of ``brain.pw``. Slots that belong to one fly
+    (``fly_of_slot``) share learning: a weight change is the mean over the fly's learning slots and
+    lands on all of its slots. Flies are kept as a CSR over slots (``_fly_ptr``, ``_fly_slots``),
+    the form the engine's fused kernels (fb_reward_step, fb_delta_apply) take; ``sign`` and
+    ``wmax`` bound every weight to [0, wmax] on its connectome sign (the cap of
+    flyzero/batch.py:141-156)."""
 
     def __init__(self, brain, cap: float, fly_of_slot=None):
         import torch
@@ -62,84 +69,94 @@ class _Plastic:
         dev = brain.device
         self.pre = torch.as_tensor(brain.pl_pre, device=dev)
         self.post = torch.as_tensor(brain.pl_post, device=dev)
-        self.w0 = torch.as_tensor(brain.w0, device=dev)
-        self.sign = torch.sign(self.w0)
-        self.wmax = np.float32(cap) * torch.maximum(torch.abs(self.w0), torch.tensor(np.float32(brain.p.w_syn), device=dev))
+        w0 = np.asarray(brain.w0, np.float32)
+        self.w0 = torch.as_tensor(w0, device=dev)
+        self.sign = torch.as_tensor(np.sign(w0).astype(np.float32), device=dev)
+        cap_w = np.float32(cap) * np.maximum(np.abs(w0), np.float32(brain.p.w_syn))
+        self.wmax = torch.as_tensor(cap_w.astype(np.float32), device=dev)
         fos = np.arange(self.B) if fly_of_slot is None else np.asarray(fly_of_slot)
         self.fly_of_slot = fos
         self.n_flies = int(fos.max()) + 1
         self._fos = torch.as_tensor(fos, device=dev)
-        order = np.argsort(fos, kind="stable")
-        self._fly_ptr = torch.as_tensor(np.r_[0, np.cumsum(np.bincount(fos, minlength=self.n_flies))].astype(np.int32),
-                                        device=dev)
-        self._fly_slots = torch.as_tensor(order.astype(np.int32), device=dev)
+        per_fly = np.bincount(fos, minlength=self.n_flies)
+        self._fly_ptr = torch.as_tensor(np.concatenate([[0], np.cumsum(per_fly)]).astype(np.int32), device=dev)
+        self._fly_slots = torch.as_tensor(np.argsort(fos, kind="stable").astype(np.int32), device=dev)
+        self._slow = None
 
     def _fly_weights(self, learn: np.ndarray) -> np.ndarray:
-        """f32(1 / learning slots of the fly) per learning slot, 0 elsewhere (the onehot / n GEMM
-        operand, batch.py:161-165)."""
-        act = np.asarray(learn).astype(np.float32)
-        n = np.bincount(self.fly_of_slot, weights=act, minlength=self.n_flies).astype(np.float32)
-        return (act / np.maximum(n[self.fly_of_slot], np.float32(1.0))).astype(np.float32)
+        """Per slot: f32(1 / number of learning slots of its fly) if it learns, else 0."""
+        on = np.asarray(learn).astype(np.float32)
+        count = np.bincount(self.fly_of_slot, weights=on, minlength=self.n_flies).astype(np.float32)
+        return (on / np.maximum(count[self.fly_of_slot], np.float32(1.0))).astype(np.float32)
 
     def apply(self, dw, active: np.ndarray, sel=None):
-        """Average ``dw`` (slots, n_pl) over each fly's active slots; update every slot of the fly.
-        With ``sel`` (plastic indices), ``dw`` is (slots, len(sel)) and only those change."""
+        """Add to every slot the mean of ``dw`` (slots, n_pl, float32) over its fly's ``active``
+        slots, then clip on the sign; with ``sel`` (plastic indices) ``dw`` is (slots, len(sel)) and
+        only those weights change. One fb_delta_apply launch: ``dw`` enters as the trace, the
+        per-slot mean weight as the coefficient and a unit error, so the kernel's per-fly sum is the
+        average (summed in slot order)."""
         import torch
 
-        dev = self.brain.device
-        onehot = torch.zeros((self.n_flies, self.B), dtype=torch.float32, device=dev)
-        onehot[self._fos, torch.arange(self.B, device=dev)] = torch.as_tensor(np.asarray(active, np.float32), device=dev)
-        n = onehot.sum(1, keepdim=True)
-        dw = torch.as_tensor(dw, device=dev)
-        per_fly = (onehot / torch.clamp(n, min=1.0)).to(dw.dtype) @ dw
-        pw = self.brain.pw
-        if sel is None:
-            w = pw.to(per_fly.dtype) + per_fly[self._fos]
-            pw[...] = (self.sign * torch.minimum(torch.clamp(self.sign * w, min=0.0), self.wmax)).to(pw.dtype)
-        else:
-            sel = torch.as_tensor(sel, device=dev)
-            sign, wmax = self.sign[sel], self.wmax[sel]
-            w = pw[:, sel].to(per_fly.dtype) + per_fly[self._fos]
-            pw[:, sel] = (sign * torch.minimum(torch.clamp(sign * w, min=0.0), wmax)).to(pw.dtype)
+        b = self.brain
+        dev = b.device
+        d = torch.as_tensor(dw, device=dev).to(torch.float32).contiguous()
+        idx = (torch.arange(d.shape[1], dtype=torch.int32, device=dev) if sel is None
+               else torch.as_tensor(np.asarray(sel), device=dev).to(torch.int32).contiguous())
+        if sel is None and d.shape[1] != b.pw.shape[1]:
+            raise ValueError(f"dw has {d.shape[1]} columns, the brain {b.pw.shape[1]} plastic synapses")
+        col = torch.arange(d.shape[1], dtype=torch.int32, device=dev)
+        unit = torch.ones((self.B, 1), dtype=torch.float32, device=dev)
+        zero = torch.zeros(d.shape[1], dtype=torch.int32, device=dev)
+        coef = torch.as_tensor(self._fly_weights(active), device=dev)
+        st = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+        _lib.check(b._L.fb_delta_apply(b._h, _ptr(idx), _ptr(col), _ptr(zero), d.shape[1], _ptr(d), d.shape[1],
+                                       _ptr(unit), 1, _ptr(coef), _ptr(self._fly_ptr), _ptr(self._fly_slots),
+                                       self.n_flies, _ptr(self.sign), _ptr(self.wmax), st))
 
-    # consolidation: a slow copy of every plastic synapse (and of the bias) follows the fast one
+    # Consolidation: a slow copy of the plastic weights and of the biases trails the fast ones as an
+    # exponential moving average (the fast/slow synapse pair of flyzero/batch.py:174-193).
     def consolidate(self, rate: float):
-        if getattr(self, "_slow", None) is None:
-            self._slow = (self.brain.pw.clone(), self.brain.bias_ext.clone())
-        self._slow[0].add_(np.float32(rate) * (self.brain.pw - self._slow[0]))
-        self._slow[1].add_(np.float32(rate) * (self.brain.bias_ext - self._slow[1]))
+        fast = (self.brain.pw, self.brain.bias_ext)
+        if self._slow is None:
+            self._slow = tuple(t.clone() for t in fast)
+        r = np.float32(rate)
+        for slow, cur in zip(self._slow, fast):
+            slow.add_((cur - slow) * r)
 
     def swap_slow(self):
         """Exchange the fast and the consolidated weights (call again to swap back)."""
-        if getattr(self, "_slow", None) is None:
-            return
-        pw, bias = self._slow
-        fast = (self.brain.pw.clone(), self.brain.bias_ext.clone())
-        self.brain.pw.copy_(pw)
-        self.brain.bias_ext.copy_(bias)
-        self._slow = fast
+        if self._slow is not None:
+            held = tuple(t.clone() for t in (self.brain.pw, self.brain.bias_ext))
+            self.brain.pw.copy_(self._slow[0])
+            self.brain.bias_ext.copy_(self._slow[1])
+            self._slow = held
 
     def state(self, fly: int) -> dict:
-        slot = int(np.flatnonzero(self.fly_of_slot == fly)[0])
-        return {"pos": self.brain.plastic_pos.astype(np.int32), "data": self.brain.pw[slot].cpu().numpy(),
+        """The fly's weights in the reference's npz layout {pos, data, w0}."""
+        first = int(np.argmax(self.fly_of_slot == fly))
+        return {"pos": self.brain.plastic_pos.astype(np.int32), "data": self.brain.pw[first].cpu().numpy(),
                 "w0": self.w0.cpu().numpy()}
 
     def load(self, st: dict, flies=None):
-        """Load weights saved by this class or by the single-instance rules (entries matched by CSR
-        position; positions not in the file keep their connectome values), batch.py:203-212."""
+        """Weights saved by this class or by the single-instance rules, matched by CSR position;
+        plastic synapses the file does not name start from their connectome weight."""
         import torch
 
-        pos = self.brain.plastic_pos
-        vals = self.w0.cpu().numpy().copy()
-        where = np.searchsorted(pos, st["pos"])
-        ok = (where < len(pos)) & (pos[np.minimum(where, len(pos) - 1)] == st["pos"])
-        vals[where[ok]] = np.asarray(st["data"])[ok]
+        mine = np.asarray(self.brain.plastic_pos, np.int64)
+        _, at_mine, at_file = np.intersect1d(mine, np.asarray(st["pos"], np.int64), assume_unique=True,
+                                             return_indices=True)
+        row = self.w0.cpu().numpy().copy()
+        row[at_mine] = np.asarray(st["data"], np.float32)[at_file]
         slots = np.arange(self.B) if flies is None else np.flatnonzero(np.isin(self.fly_of_slot, flies))
-        self.brain.pw[torch.as_tensor(slots, device=self.brain.device)] = torch.as_tensor(vals, device=self.brain.device)
+        dev = self.brain.device
+        self.brain.pw.index_copy_(0, torch.as_tensor(slots, device=dev),
+                                  torch.as_tensor(row, device=dev).expand(len(slots), -1).contiguous())
 
     def drift(self) -> np.ndarray:
-        """Mean relative change from the connectome, per slot."""
-        return (self.brain.pw - self.w0).abs().div(self.wmax).mean(1).cpu().numpy()
+        """Per slot: mean over the plastic synapses of |w - w0| / wmax."""
+        import torch
+
+        return torch.mean(torch.abs(self.brain.pw - self.w0) / self.wmax, dim=1).cpu().numpy()
 
 
 class BatchReward(_Plastic):
@@ -162,6 +179,9 @@ class BatchReward(_Plastic):
         self.noise = np.zeros((self.B, len(self.targets)))
         self._coef = torch.zeros(self.B, dtype=torch.float64, device=dev)
         self._fw = torch.zeros(self.B, dtype=torch.float32, device=dev)
+        # the per-window scalars reach the device through pinned buffers: a step never blocks the host
+        self._coef_in = _lib.HostStage(self.B, torch.float64)
+        self._fw_in = _lib.HostStage(self.B, torch.float32)
 
     def reset(self, slots):
         s = np.atleast_1d(slots)
@@ -174,9 +194,13 @@ class BatchReward(_Plastic):
         return torch.as_tensor(np.asarray(s), device=self.brain.device)
 
     def exploration(self, window_ms: float) -> np.ndarray:
-        """Extra Poisson rates (slots, len(self.targets)) for the target neurons."""
-        a = window_ms / self.p.noise_tau_ms
-        self.noise += -a * self.noise + np.sqrt(2 * a) * self.rng.standard_normal(self.noise.shape)
+        """Extra Poisson rates (slots, len(self.targets)) for the target neurons: one Euler step of
+        an Ornstein-Uhlenbeck process per window (time constant noise_tau_ms, unit stationary
+        variance), rectified and scaled by noise_hz. The float64 operations and the generator's
+        draws are those of flyzero/batch.py:476-480, so equal seeds give the reference's drive."""
+        h = window_ms / self.p.noise_tau_ms
+        shock = np.sqrt(2 * h) * self.rng.standard_normal(self.noise.shape)
+        self.noise += shock - h * self.noise
         return np.maximum(self.p.noise_hz * self.noise, 0.0)
 
     def _run(self, counts, coef, learn, window_ms):
@@ -186,13 +210,14 @@ class BatchReward(_Plastic):
         ae = np.exp(-window_ms / p.tau_elig_ms)
         ap = 1 - np.exp(-window_ms / p.tau_post_ms)
         apply = bool(np.asarray(learn).any())
-        self._coef.copy_(torch.as_tensor(coef, dtype=torch.float64))
-        self._fw.copy_(torch.as_tensor(self._fly_weights(learn)))
         b = self.brain
+        stream = torch.cuda.current_stream(b.device)
+        self._coef_in.put(self._coef, np.asarray(coef, np.float64))
+        self._fw_in.put(self._fw, self._fly_weights(learn))
         _lib.check(b._L.fb_reward_step(b._h, _ptr(counts), _ptr(self.elig), _ptr(self.post_mean), _ptr(self._coef),
                                        _ptr(self._fly_ptr), _ptr(self._fly_slots), _ptr(self._fw), self.n_flies, None,
                                        float(ae), float(ap), float(np.float32(p.cap)), int(apply),
-                                       C.c_void_p(torch.cuda.current_stream(b.device).cuda_stream)))
+                                       C.c_void_p(stream.cuda_stream)))
 
     def step(self, counts, reward: np.ndarray, learn: np.ndarray, window_ms: float):
         """``counts``: device (slots, n) int32 of the window just run; ``reward``: (slots,);

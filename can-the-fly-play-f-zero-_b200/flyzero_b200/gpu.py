@@ -231,8 +231,17 @@ class BatchBrain:
         import torch
 
         s = np.asarray(steps_per_instance, np.int64)
-        stop = np.where(s < 0, np.iinfo(np.int64).max, self.t + s)
-        self.stop_tick.copy_(torch.as_tensor(stop, device=self.device))
+        self.set_stop_tick(np.where(s < 0, np.iinfo(np.int64).max, self.t + s))
+
+    def set_stop_tick(self, ticks):
+        """Instance b advances until the engine's tick reaches ``ticks[b]`` (absolute ticks, as
+        ``t`` counts them). Enqueued on the current stream through pinned staging: the host is
+        not synchronised."""
+        import torch
+
+        if getattr(self, "_stop_in", None) is None:
+            self._stop_in = _lib.HostStage(self.B, torch.int64)
+        self._stop_in.put(self.stop_tick, np.asarray(ticks, np.int64))
 
     # ---- schedule autotuner -------------------------------------------------------------------
     def schedule_candidates(self):

@@ -110,12 +110,14 @@ class BatchMotor:
         return [self.buttons(r, k) for k, r in enumerate(rates)]
 
     def _tap(self, k, j, x, threshold, span):
-        """+1 (left), -1 (right) or 0 this frame; duty = (|x| - threshold) / span (batch.py:113-119)."""
-        duty = np.sign(x) * np.clip((abs(x) - threshold) / span, 0.0, 1.0)
-        self.acc[k, j] += duty
-        t = 1 if self.acc[k, j] >= 0.5 else -1 if self.acc[k, j] <= -0.5 else 0
-        self.acc[k, j] -= t
-        return t
+        """Pulse-density modulation of a steering command: a first-order sigma-delta quantiser.
+        The command's duty, clip((|x| - threshold) / span, 0, 1) with the sign of x, is integrated
+        per (slot k, axis j); a frame emits +1 or -1 when the integral reaches +-0.5 and subtracts
+        it, else 0. The button timing must equal flyzero/batch.py:113-119 frame for frame."""
+        level = self.acc[k, j] + np.clip((abs(x) - threshold) / span, 0.0, 1.0) * np.sign(x)
+        tap = int(level >= 0.5) - int(level <= -0.5)
+        self.acc[k, j] = level - tap
+        return tap
 
     def buttons(self, r, k: int = 0) -> dict:
         """Buttons of one slot from its smoothed rates (batch.py:121-138)."""

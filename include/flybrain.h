@@ -4,7 +4,7 @@
  * share one connectome. It replaces the reference's CPU engine `flyzero.brain.Brain`
  * (flyzero/brain.py:79-172) and its CuPy engine `flyzero.gpu.BatchBrain`
  * (flyzero/gpu.py:131-254); the reference binds its engines from Python, so the binding a
- * maintainer adds is a ctypes stub (INTEGRATION.md shows it).
+ * maintainer adds is a ctypes stub over these entry points.
  *
  * Conventions
  *   - Every function returns FB_OK (0) or an FB_ERR_* code; fb_last_error() gives the message
@@ -122,7 +122,9 @@ int fb_set_plastic(fb_brain* brain, const int64_t* pos /*[host]*/, int64_t count
 
 /* Back to rest: v = v_rest, g = 0, ref = 0 and no synaptic input in flight
  * (BatchBrain.reset, flyzero/gpu.py:186-199; Brain.reset, flyzero/brain.py:104-110).
- * flies == NULL or n_flies < 0: every instance, and t = 0. Plastic weights are kept. */
+ * flies == NULL or n_flies < 0: every instance, and t = 0. Plastic weights are kept. The list
+ * of flies is copied before return (through pinned staging; the host is not synchronised with the
+ * stream). */
 int fb_reset(fb_brain* brain, const int32_t* flies /*[host]*/, int32_t n_flies, void* stream);
 
 /* Advance every instance `steps` steps (BatchBrain.run, flyzero/gpu.py:228-254; Brain.run,
@@ -265,8 +267,11 @@ int fb_check(fb_brain* brain, void* stream);
  * clear != 0 zeroes the in-flight input first (start of a simulation); clear == 0 continues the
  * previous call's simulation. Calls that overlap on the GPU (other streams, other threads) race
  * on the array. The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture. No cudaMalloc, cudaFree
- * or allocating library routine is called. */
+ * (cudaGetSymbolAddress); make that first call before any stream capture. A device reset
+ * (cudaDeviceReset) may move the array: the address looked up before it is stale afterwards, so do
+ * not call this entry point again in a process that reset the device. t0 must be >= 0, and
+ * delay/dt, t_ref/dt finite and at most 1e6 (else FB_ERR_ARG before any device work). No
+ * cudaMalloc, cudaFree or allocating library routine is called. */
 #define FB_STATIC_RING_ENTRIES 1048576
 int fb_run_static(const fb_params* params, int64_t n, const int64_t* indptr, const int32_t* indices,
                   const float* weights, float* v, float* g, int8_t* ref, const int32_t* ext_idx,

@@ -41,3 +41,31 @@ def test_errors_cross_the_boundary_as_codes():
     assert rc == _lib.FB_ERR_ARG
     assert "bad connectome arguments" in _lib.last_error()
     assert lib.fb_get_info(None, None) == _lib.FB_ERR_ARG
+
+
+def test_static_run_rejects_bad_ticks_and_delays_before_any_device_work():
+    """fb_run_static checks its scalar arguments on the host and returns FB_ERR_ARG before it
+    touches the device, so these cases run without a GPU (the buffers are never dereferenced)."""
+    import math
+
+    from flyzero_b200 import _lib
+    from flyzero_b200.brain import LIFParams
+
+    lib = _lib.load()
+    buf = (C.c_int64 * 8)()
+    b = C.cast(buf, C.c_void_p)
+
+    def call(params, t0=0, steps=1, n=4):
+        prm = _lib.Params(**{k: float(getattr(params, k)) for k, _ in _lib.Params._fields_})
+        return lib.fb_run_static(C.byref(prm), n, b, b, b, b, b, b, None, None, None, 0, 0, t0, steps, 1, b, None)
+
+    p = LIFParams()
+    assert call(p, t0=-1) == _lib.FB_ERR_ARG
+    assert "t0" in _lib.last_error()
+    assert call(p, t0=2 ** 63 - 1, steps=5) == _lib.FB_ERR_ARG
+    for bad in (LIFParams(delay=math.nan), LIFParams(delay=math.inf), LIFParams(delay=1e300),
+                LIFParams(delay=-1e300), LIFParams(t_ref=math.nan), LIFParams(t_ref=-5.0), LIFParams(dt=math.inf)):
+        assert call(bad) == _lib.FB_ERR_ARG, bad
+    # n * (n_delay + 1) beyond the array, including sizes whose product overflows int64
+    assert call(p, n=2 ** 40) == _lib.FB_ERR_ARG
+    assert "exceeds the static ring" in _lib.last_error()

@@ -32,3 +32,38 @@ def test_reference_arm_json_line():
 def test_fleet_reference_arm_is_marked_unavailable():
     d = _run("--impl", "reference", "--component", "fleet", "--steps", "1", "--warmup", "1")
     assert d["impl"] == "reference" and "unavailable" in d
+
+
+def test_episode_bookkeeping_restarts_runs_inside_the_window():
+    """The batched workload's runs: staggered starts make runs end inside a 30-frame window, ended
+    instances are restarted with a new U{0.5,1,2,3} s length, and the active steps per frame are the
+    ones the engine's run-length masking lets through."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    import bench
+    from flyzero_b200 import workloads as wl
+
+    work = wl.BatchedWorkload.make(64, seed=0)
+    ep = bench.Episodes(work, seed=23)
+    first = (work.run_ms / bench.DT).astype(np.int64)
+    assert np.all(ep.stop >= 1) and np.all(ep.stop <= first)
+    t, restarted, partial = 0, 0, 0
+    for _ in range(33):
+        ended = ep.frame(t)
+        assert np.all(ep.stop[ended] - t >= 5000)
+        assert np.all(np.isin(ep.stop[ended] - t, bench.Episodes.LENGTHS))
+        act = ep.active(t, 166)
+        assert np.all((act >= 0) & (act <= 166))
+        partial += int(np.sum((act > 0) & (act < 166)))
+        restarted += len(ended)
+        t += 166
+    assert restarted > 0 and partial > 0
+
+
+def test_dram_traffic_comes_from_the_committed_profile():
+    sys.path.insert(0, ROOT)
+    import bench
+
+    traffic, src = bench.dram_traffic_record()
+    assert traffic and traffic > 1e8 and "commit" in src

@@ -151,3 +151,41 @@ def test_plastic_state_round_trips_through_npz(torch, tmp_path):
     np.testing.assert_array_equal(got[:, k], np.tile(back["data"], (2, 1)))
     rest = np.setdiff1d(np.arange(len(pos2)), k)
     np.testing.assert_array_equal(got[:, rest], np.tile(gb2.w0[rest], (2, 1)))
+
+
+@pytest.mark.parametrize("with_sel", [False, True])
+def test_plastic_apply_averages_over_each_flys_active_slots(torch, with_sel):
+    """_Plastic.apply (batch.py:158-172) for an arbitrary dw: every slot of a fly gets the mean of
+    dw over the fly's active slots, clipped on the connectome sign to [0, wmax]; with ``sel`` only
+    those synapses move. Compared with the plain NumPy formula (float32; the per-fly sum's order
+    is the only freedom, hence the tolerance)."""
+    from flyzero_b200.batch import BatchReward
+
+    gb, rng, targets, fos = _batch_setup(torch)
+    br = BatchReward(gb, fly_of_slot=fos, targets=targets)
+    n_pl = gb.pw.shape[1]
+    sel = np.sort(rng.choice(n_pl, n_pl // 3, replace=False)) if with_sel else None
+    cols = n_pl if sel is None else len(sel)
+    w = gb.pw.cpu().numpy().copy()
+    sign = np.sign(gb.w0).astype(np.float32)
+    wmax = (np.float32(3.0) * np.maximum(np.abs(gb.w0), np.float32(gb.p.w_syn))).astype(np.float32)
+    for f in range(4):
+        dw = (rng.standard_normal((gb.B, cols)) * 0.2).astype(np.float32)
+        active = rng.random(gb.B) < 0.6
+        br.apply(torch.as_tensor(dw, device=gb.device), active, sel)
+        onehot = np.zeros((int(fos.max()) + 1, gb.B), np.float32)
+        onehot[fos, np.arange(gb.B)] = active
+        per_fly = (onehot / np.maximum(onehot.sum(1, keepdims=True), 1)) @ dw
+        k = np.arange(n_pl) if sel is None else sel
+        cand = w[:, k] + per_fly[fos]
+        w[:, k] = sign[k] * np.clip(sign[k] * cand, 0.0, wmax[k])
+        np.testing.assert_allclose(gb.pw.cpu().numpy(), w, rtol=1e-6, atol=1e-7)
+    if sel is not None:
+        rest = np.setdiff1d(np.arange(n_pl), sel)
+        np.testing.assert_array_equal(gb.pw.cpu().numpy()[:, rest], np.tile(gb.w0[rest], (gb.B, 1)))
+    before = br.drift()
+    assert before.shape == (gb.B,) and before.max() > 0
+    br.consolidate(0.5)
+    br.swap_slow()
+    br.swap_slow()
+    np.testing.assert_array_equal(br.drift(), before)

@@ -106,3 +106,57 @@ def _lib_limit(L):
 
     text = open(os.path.join(ROOT, "include", "flybrain.h")).read()
     return int(re.search(r"#define FB_STATIC_RING_ENTRIES (\d+)", text).group(1))
+
+
+def _static_vs_engine(torch, conn, p, steps, with_inputs):
+    """Run one instance through fb_run_static and through BatchBrain (Q32.32 mode) and compare."""
+    from flyzero_b200 import _lib
+    from flyzero_b200.gpu import BatchBrain
+
+    L = _lib.load()
+    n = conn.n
+    gb = BatchBrain(conn.weights, p, batch=1, seed=9, fixed_point=True)
+    if with_inputs:
+        idx, rate = wl.config1_inputs(n, seed=4)
+        gb.set_input(idx, rate * 3)
+    else:                                   # no ext slots: a depolarised, seeded start makes the net fire
+        gen = torch.Generator(device=gb.device).manual_seed(5)
+        gb.v.copy_(torch.rand(gb.v.shape, generator=gen, device=gb.device) * 8.0 + p.v_rest)
+        gb.g.copy_(torch.rand(gb.g.shape, generator=gen, device=gb.device) * 10.0)
+    dev = gb.device
+    indptr = torch.as_tensor(gb.indptr, device=dev)
+    indices = torch.as_tensor(gb.indices, device=dev)
+    weights = torch.as_tensor(gb.data, device=dev)
+    v, g, ref = gb.v[0].clone(), gb.g[0].clone(), gb.ref[0].clone()
+    counts = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    ext = (_ptr(gb.d_ext_idx), _ptr(gb.p_ext), _ptr(gb.bias_ext)) if with_inputs else (None, None, None)
+    for call in range(2):
+        rc = L.fb_run_static(C.byref(_params(p)), n, _ptr(indptr), _ptr(indices), _ptr(weights), _ptr(v), _ptr(g),
+                             _ptr(ref), *ext, 9, call * steps, call * steps, steps, 1 if call == 0 else 0,
+                             _ptr(counts), stream)
+        assert rc == _lib.FB_OK, _lib.last_error()
+        want = gb.run_steps(steps)[0]
+        torch.cuda.synchronize(dev)
+        if call == 0:
+            assert int(want.sum()) > 0
+        assert torch.equal(counts, want), f"call {call}: spike counts differ"
+        assert torch.equal(v, gb.v[0]) and torch.equal(g, gb.g[0]) and torch.equal(ref, gb.ref[0]), \
+            f"call {call}: state differs"
+
+
+def test_static_run_without_ext_inputs(torch):
+    from flyzero_b200.brain import LIFParams
+
+    _static_vs_engine(torch, cx.synthetic(4096, seed=6), LIFParams(), 150, with_inputs=False)
+
+
+def test_static_run_at_the_exact_array_limit(torch):
+    """n * (n_delay + 1) equal to the array's size: 65,536 neurons with a 1.5 ms delay (16 slots)."""
+    from flyzero_b200 import _lib
+    from flyzero_b200.brain import LIFParams
+
+    p = LIFParams(delay=1.5)
+    n = _lib_limit(_lib.load()) // 16
+    assert n == 65536 and max(1, round(p.delay / p.dt)) + 1 == 16
+    _static_vs_engine(torch, cx.synthetic(n, seed=8), p, 120, with_inputs=True)
