@@ -365,6 +365,7 @@ class FrameLoop:
         self.resets = 0
         self.reset_instances = 0
         self.public = False           # True: BatchBrain.run(ms), the reference's call
+        self.run_launches = 0         # the engine's launches inside the runs alone
         gb.set_stop_tick(self.ep.stop)
 
     def __call__(self, f: int, write_rates, counts=None, events=None):
@@ -381,7 +382,9 @@ class FrameLoop:
         write_rates(f)
         if events:
             events[0].record()
+        l0 = gb.launches
         c = gb.run(self.fs * DT) if self.public else gb.run_steps(self.fs, counts=counts)
+        self.run_launches += gb.launches - l0
         if events:
             events[1].record()
         self.br.step(c, self.rewards[f], act > 0, self.fs * DT)
@@ -439,13 +442,11 @@ def run_ours(args, world, rank, local):
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     e_all0, e_all1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     active = 0
-    l_run = 0
+    l_run0 = loop.run_launches
     e_all0.record(st)
     for k in range(args.steps):
         f = args.warmup + k
-        l0 = gb.launches
         _, a = loop(f, rates, counts[f], events=ev[k])     # events around the run's launches
-        l_run += gb.launches - l0
         active += a
     e_all1.record(st)
     torch.cuda.synchronize(dev)
@@ -462,7 +463,7 @@ def run_ours(args, world, rank, local):
     alg_bytes = BYTES_PER_NEURON_STEP * neuron_steps + BYTES_PER_SPIKE * spk + BYTES_PER_EDGE * edges
     info = gb.info()
     peak, peak_kind = peaks()
-    n_kern = max(1, l_run)      # the engine's launches inside the runs: one per instance group per frame
+    n_kern = max(1, loop.run_launches - l_run0)   # the runs' launches: one per instance group per frame
     achieved = (alg_bytes / n_kern) / (run_ms / 1000.0 / n_kern) / 1e9
     traffic, traffic_src = dram_traffic_record()
     out = {
