@@ -54,9 +54,10 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
     ap.add_argument("--engine", default="auto", choices=["auto", "step", "persistent"])
     ap.add_argument("--lanes", type=int, default=0, help="lanes per spike work item (8/16/32; 0 = default)")
-    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet"],
+    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet", "tune"],
                     help="brain: the LIF engine (default); eye: the motion eye front end alone; fleet: the "
-                         "whole frame loop (frames -> eye -> brain -> readout) through the public API")
+                         "whole frame loop (frames -> eye -> brain -> readout) through the public API; "
+                         "tune: the surrogate-screened interface search at full scale (one run)")
     return ap.parse_args()
 
 
@@ -843,11 +844,52 @@ def run_fleet(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+TUNE_METRIC = "surrogate DN-count error on the simulated survivors, last CMA-ES generation (138k LIF, 1,024 screened / 64 simulated)"
+
+
+def run_tune(args, world, rank, local):
+    """The learned surrogate at full scale (config 5): 200,000 frames from the B=64 engine, the
+    BF16 MLP trained on the device, then CMA-ES over the 12-parameter interface with 1,024
+    candidates screened and 64 re-simulated per generation, beside CMA-ES simulating its 64
+    directly. One run (the whole search is the unit); --steps and --warmup are not used."""
+    import torch
+
+    from flyzero_b200 import tuning as T
+
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    rep = T.run(n=138_639, frames=200_000, epochs=12, generations=8, episode=30, seed=rank)
+    secs = time.perf_counter() - t0
+    log = rep["surrogate_search"]["log"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": TUNE_METRIC, "value": log[-1]["count_error"], "unit": "relative", "n_gpus": world,
+            "steps": 1, "warmup": 0, "ms_per_step": 1000 * secs, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 (surrogate) / f32+i32 (LIF)", "data": "synthetic",
+            "config": {"workload": "config 5: 200,000 frames, MLP 1280-512-512-10, 8 generations of 1,024 "
+                                   "candidates, 64 simulated at B=64, 30-frame episodes"},
+            "screened_per_simulated": log[-1]["screened"] / log[-1]["simulated"],
+            "count_error_per_generation": [g["count_error"] for g in log],
+            "count_error_uncalibrated_per_generation": [g["count_error_uncalibrated"] for g in log],
+            "best_fitness": {"surrogate": rep["surrogate_search"]["best"], "plain": rep["plain_search"]["best"]},
+            "full_simulations": {"surrogate": rep["surrogate_search"]["sims"], "plain": rep["plain_search"]["sims"],
+                                 "candidates_judged_by_surrogate": sum(g["screened"] for g in log)},
+            "train": {k: rep["train"][k] for k in ("epochs", "steps", "seconds", "tflops", "val_nll",
+                                                   "val_total_count_error")},
+            "frames_per_s": rep["frames_per_s"]}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         world = int(os.environ.get("WORLD_SIZE", "1"))
         rank = int(os.environ.get("RANK", "0"))
+        if args.component == "tune":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "component": "tune",
+                                  "unavailable": "the reference's search (flyzero/tune.py:139-166) races every "
+                                                 "candidate on its emulator, which is out of scope"}))
+            return
         if args.component == "fleet":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "component": "fleet",
@@ -858,7 +900,7 @@ def main():
         return
     world, rank, local = dist_setup(args)
     try:
-        {"eye": run_eye, "fleet": run_fleet}.get(args.component, run_ours)(args, world, rank, local)
+        {"eye": run_eye, "fleet": run_fleet, "tune": run_tune}.get(args.component, run_ours)(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -169,7 +170,9 @@ struct fb_brain {
     int64_t* pring = nullptr;
     int2* items = nullptr;
     int32_t* item_count = nullptr;
-    int64_t cap_c = 0;            // items per (step, group, segment) list
+    int64_t cap_c = 0;            // items per (step, group, segment) list (<= cap_alloc)
+    int64_t cap_alloc = 0;        // ... as allocated
+    long long barrier_cycles = BARRIER_TIMEOUT_CYCLES;   // persistent engine's grid-barrier wait budget
     int32_t list_group = 1;       // instances per group (the persistent group size, or B)
     int32_t n_groups = 1;
     int32_t n_seg = 1;            // segments per group (the persistent CTAs, or 1)
@@ -436,6 +439,7 @@ extern "C" int fb_create(const fb_params* P, const int64_t* indptr, const int32_
     h->n_seg = h->plan.group > 0 ? h->plan.ctas : 1;
     h->seg_pairs = h->plan.group > 0 ? h->plan.per : (int64_t)h->list_group * h->n_pad;
     h->cap_c = segment_capacity(H, h->n_pad, h->list_group, h->seg_pairs, h->n_seg);
+    h->cap_alloc = h->cap_c;
     TRY(dalloc(&h->items, (size_t)h->R * h->n_groups * h->n_seg * h->cap_c, tb));
     TRY(dalloc(&h->item_count, (size_t)h->R * h->n_groups * h->n_seg, tb));
     TRY(dalloc(&h->reset_tick, (size_t)batch, tb));
@@ -814,6 +818,17 @@ extern "C" int fb_set_trace(fb_brain* h, long long* trace, int64_t capacity)
     return FB_OK;
 }
 
+extern "C" int fb_set_limits(fb_brain* h, int64_t barrier_cycles, int64_t item_capacity)
+{
+    if (!h) return fail(FB_ERR_ARG, "NULL brain");
+    if (barrier_cycles < 0 || item_capacity < 0 || item_capacity > h->cap_alloc)
+        return fail(FB_ERR_ARG, "barrier_cycles %lld and item_capacity %lld must be >= 0, the capacity at most %lld",
+                    (long long)barrier_cycles, (long long)item_capacity, (long long)h->cap_alloc);
+    h->barrier_cycles = barrier_cycles ? (long long)barrier_cycles : BARRIER_TIMEOUT_CYCLES;
+    h->cap_c = item_capacity ? item_capacity : h->cap_alloc;
+    return FB_OK;
+}
+
 extern "C" int fb_check(fb_brain* h, void* stream)
 {
     if (!h) return fail(FB_ERR_ARG, "NULL brain");
@@ -922,6 +937,11 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         P.trace = ((int64_t)steps * h->plan.ctas * TRACE_SLOTS <= h->trace_cap) ? h->trace : nullptr;
         P.pushed_until = h->pushed_until;
         P.epoch = h->epoch;
+        P.barrier_cycles = h->barrier_cycles;
+        {
+            const char* gv = std::getenv("FLYBRAIN_PUSH_GATE");   // A/B of the push gate (temporary)
+            P.push_gate = gv ? std::atoi(gv) : 1;
+        }
         CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
         int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
                                    record, h->lanes, st);

@@ -67,6 +67,7 @@ SIGNATURES = {
     "fb_run": (C.c_int, [vp, C.c_int32, vp, vp, vp, vp, vp]),
     "fb_set_schedule": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32]),
     "fb_set_trace": (C.c_int, [vp, vp, C.c_int64]),
+    "fb_set_limits": (C.c_int, [vp, C.c_int64, C.c_int64]),
     "fb_trace_rates": (C.c_int, [vp, vp, vp, C.c_int32, vp, C.c_float, C.c_float, vp, C.c_int32, vp, C.c_float,
                                  C.c_float, vp]),
     "fb_delta_apply": (C.c_int, [vp, vp, vp, vp, C.c_int32, vp, C.c_int32, vp, C.c_int32, vp, vp, vp, C.c_int32, vp,

@@ -6,7 +6,8 @@ mismatch (the horizon over which the FP32 raster equals the FP64 one), and the p
 error over the run. Both engines step together one step at a time; all comparisons stay on the
 device until the end.
 
-Run as a script for the high-activity workload (5 % of neurons at 150 Hz Poisson, B=16):
+Run as a script for the high-activity workload (5 % of neurons at 210 Hz Poisson, B=16); it also
+reports which schedule (engine, push or pull propagation) the autotuner picks at that activity:
 
     python -m flyzero_b200.precision --n 138639 --batch 16 --steps 10000
 """
@@ -99,7 +100,22 @@ def main(argv=None):
     conn = cx.flywire_scale() if args.n == 138_639 else cx.synthetic(args.n, seed=args.seed)
     idx, rate = wl.high_activity_inputs(conn.n, seed=args.seed)
     rep = precision_report(conn.weights, LIFParams(dt=0.1), args.batch, idx, rate, args.steps, seed=args.seed)
+    rep["schedule"] = schedule_at_activity(conn.weights, LIFParams(dt=0.1), args.batch, idx, rate, seed=args.seed)
     print(json.dumps(rep))
+
+
+def schedule_at_activity(weights, params, batch, inputs, rate_hz, seed: int = 0, warm: int = 1000,
+                         steps: int = 166) -> dict:
+    """The autotuner's choice on this workload once its activity has settled: every schedule
+    (persistent, step engine with push, step engine with pull) timed on the running simulation."""
+    from .gpu import BatchBrain
+
+    b = BatchBrain(weights, params, batch=batch, seed=seed)
+    b.set_input(inputs, rate_hz)
+    b.run_steps(warm)
+    rep = b.autotune(steps=steps)
+    rep["best"] = "/".join(map(str, rep["best"]))
+    return rep
 
 
 if __name__ == "__main__":

@@ -93,8 +93,12 @@ class BatchedWorkload:
         return out
 
 
-def high_activity_inputs(n: int, seed: int = 0, frac: float = 0.05, rate_hz: float = 150.0):
-    """5% of neurons at 150 Hz Poisson (the precision / high-activity workload)."""
+def high_activity_inputs(n: int, seed: int = 0, frac: float = 0.05, rate_hz: float = 210.0):
+    """5% of neurons Poisson-driven at 210 Hz (the precision / high-activity workload). On the
+    seeded 138,639-neuron synthetic graph this is the strongest drive of 5% whose activity stays
+    put: ~15 Hz mean over 1 s (~210 spikes per step per instance); 150 Hz gives 8 Hz, and from
+    ~220 Hz (or 7.8% at 150 Hz) the network ignites within 0.4 s to ~196 Hz, every neuron firing
+    as fast as its refractory period allows (measured with the CPU restatement, 10,000 steps)."""
     rng = np.random.default_rng(seed + 32452843)
     idx = np.sort(rng.choice(n, int(round(frac * n)), replace=False)).astype(np.int64)
     return idx, np.full(len(idx), rate_hz, np.float32)

@@ -241,6 +241,16 @@ int fb_set_schedule(fb_brain* brain, int32_t engine, int32_t propagation, int32_
  * counterpart in the reference. */
 int fb_set_trace(fb_brain* brain, long long* trace, int64_t capacity);
 
+/* Limits for fault drills (diagnostics; no counterpart in the reference, whose only guard is a
+ * capacity assert, flyzero/gpu.py:166-168). barrier_cycles: the persistent engine's grid-barrier
+ * wait budget in SM clock cycles before it gives up, raises FB_ERR_TIMEOUT (fb_check) and every CTA
+ * returns (0: the default, about 4 s). item_capacity: work items per spike list, at most the
+ * allocated capacity fb_get_info reports; a smaller one makes an active run raise FB_ERR_OVERFLOW
+ * (items beyond it are dropped, never written out of bounds; 0: the allocated capacity). The list
+ * layout depends on it: change it only right after fb_reset of every instance. A run that timed
+ * out or overflowed leaves the simulation invalid: fb_reset it. */
+int fb_set_limits(fb_brain* brain, int64_t barrier_cycles, int64_t item_capacity);
+
 /* Device error flags raised since the last call (overflow, barrier timeout), then cleared.
  * Synchronises `stream`. Returns FB_OK or the first raised FB_ERR_* code. */
 int fb_check(fb_brain* brain, void* stream);

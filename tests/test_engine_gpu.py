@@ -304,21 +304,25 @@ def test_lanes_per_item_agree(torch, lanes):
 
 
 def test_fp64_oracle_mode(torch, golden):
-    """FP64 state on the GPU: bit-exact vs the oracle's FP64 engine semantics, raster-exact vs the
-    reference kernel re-jitted on float64 (workload 1, first 4,000 steps)."""
+    """FP64 state on the GPU over the whole config-1 run (10,000 steps of the 16,384-neuron
+    workload): bit-exact vs the oracle's FP64 engine semantics; raster-exact at every step, equal
+    counts and final voltages within V_TOL vs the reference kernel re-jitted on float64
+    (flyzero/brain.py:32-58)."""
     from flyzero_b200.brain import LIFParams
 
     g = golden("workload_n16384.npz")
     conn = cx.synthetic(16_384, seed=1)
     idx, rate = wl.config1_inputs(conn.n, seed=1)
-    steps = 4000
+    steps = 10_000
     kicks = O.reference_kicks(int(g["seed_k"]), 10_000, rate * np.float32(0.1 / 1000.0))[:steps]
     gb = _bb(conn.weights, LIFParams(), 1, "step", fp64=True)
     gb.slots(idx)
     kr = np.zeros((steps, 1, gb.p_ext.shape[1]), bool)
     kr[:, 0, gb._slot[idx]] = kicks
-    _, _, sd = gb.run_steps(steps, _raster(torch, kr, gb.device), record=True)
+    c, _, sd = gb.run_steps(steps, _raster(torch, kr, gb.device), record=True)
     np.testing.assert_array_equal(sd.cpu().numpy().view(np.uint64)[:, 0], g["f64_step_digest"][:steps])
+    np.testing.assert_array_equal(c.cpu().numpy()[0], g["f64_counts"])
+    assert np.abs(gb.v.cpu().numpy()[0] - g["f64_v"]).max() <= V_TOL
     eo = O.EngineOracle(conn.weights, O.Params(), batch=1, real=np.float64)
     eo.slots(idx)
     eo.run_steps(steps, kr)

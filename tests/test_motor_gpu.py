@@ -90,3 +90,27 @@ def test_clamp_controller_and_bias(torch):
         np.testing.assert_allclose(c.u.cpu().numpy(), u, rtol=1e-5, atol=1e-5)
         np.testing.assert_allclose(gb.bias_ext[:, gb.slots(idx).long()].cpu().numpy(), base + applied, rtol=1e-5, atol=1e-5)
     assert np.abs(u).max() > 0.1
+
+
+def test_batch_motor_matches_the_reference_readout(torch, golden):
+    """Every slot of BatchMotor against the reference's own MotorReadout.update
+    (flyzero/motor.py:78-95, tests/golden/motor.npz from make_motor_golden.py): smoothed rates within
+    float32 rounding of the reference's float64 (relative 1e-5), the buttons equal, frame by frame;
+    one readout group is empty, as a cell type missing from the connectome would be."""
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+    from flyzero_b200.motor import READOUT, BatchMotor, MotorParams
+
+    g = golden("motor.npz")
+    cnt = g["counts"]
+    frames, slots, n = cnt.shape
+    groups = {name: g["group_" + name] for name in READOUT}
+    assert min(len(v) for v in groups.values()) == 0
+    gb = BatchBrain(sp.identity(n, dtype=np.float32, format="csr"), LIFParams(), batch=slots)
+    m = BatchMotor(gb, groups, MotorParams())
+    names = [str(x) for x in g["button_names"]]
+    for f in range(frames):
+        btn = m.update(torch.as_tensor(cnt[f], device="cuda"), float(g["window"]))
+        np.testing.assert_allclose(m.rates, g["rates"][f], rtol=1e-5, atol=1e-4)
+        got = np.array([[b[k] for k in names] for b in btn])
+        np.testing.assert_array_equal(got, g["buttons"][f], err_msg=f"frame {f}")

@@ -109,7 +109,9 @@ def test_surrogate_screening_gains_over_plain_search(torch):
     """End to end on a 16,384-neuron graph: frames from the engine, training, then CMA-ES with the
     surrogate pre-screen (1,024 screened, 64 simulated per generation) against CMA-ES that
     simulates its 64 candidates directly - same number of full simulations. The screened search
-    reaches the better interface, and its surrogate is within tolerance by the last generation."""
+    reaches the better interface, and once calibrated on the survivors of a generation the
+    surrogate's DN counts are within 5 % of the simulated ones in the last
+    generation."""
     from flyzero_b200 import tuning as T
 
     rep = T.run(n=16384, frames=20480, epochs=4, generations=4, episode=30, seed=0)
@@ -117,4 +119,5 @@ def test_surrogate_screening_gains_over_plain_search(torch):
     assert s["sims"] == p["sims"] == 4 * 64
     assert all(g["screened"] / g["simulated"] >= 10 for g in s["log"])
     assert s["best"] >= p["best"], (s["best"], p["best"])
-    assert s["log"][-1]["count_error"] < 0.25
+    assert s["log"][-1]["count_error"] <= 0.05, [g["count_error"] for g in s["log"]]
+    assert all(g["count_error"] <= g["count_error_uncalibrated"] + 0.05 for g in s["log"][1:])
