@@ -500,11 +500,42 @@ def run_ours(args, world, rank, local):
     }
     if not args.no_extras:
         out["plain_b1"] = plain_b1(conn, drive, dev)
+        out["persistent_b1"] = persistent_b1(conn, drive, dev)
         out["e2e"] = e2e(conn, work, drive, host_rates, args, fs, n_in, inv, dev, rank, pos)
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(conn, drive, args.cpu_seconds)
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def persistent_b1(conn, drive, dev, frames: int = 6):
+    """One instance on the persistent engine (the drop-in for the game loop's Brain.run,
+    flyzero/brain.py:133-172): B=1, one cooperative launch per 166-step frame."""
+    import torch
+
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=1, seed=5)
+    if gb.info().group == 0:
+        return None
+    gb.set_schedule("persistent")
+    gb.set_input(np.r_[drive.inputs, drive.tonic], np.r_[wl.grating_rates(drive, 0.0, 0.4), 60.0])
+    fs = wl.frame_steps(DT)
+    for _ in range(2):
+        gb.run_steps(fs)
+    torch.cuda.synchronize(dev)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = torch.cuda.current_stream(dev)
+    a.record(st)
+    for _ in range(frames):
+        c = gb.run_steps(fs)
+    b.record(st)
+    torch.cuda.synchronize(dev)
+    ms = a.elapsed_time(b)
+    return {"value": frames * fs * conn.n / (ms / 1000.0), "unit": UNIT, "engine": "persistent, B=1, 1 launch/frame",
+            "ms_per_frame": ms / frames, "spikes_last_frame": int(c.sum())}
 
 
 def plain_b1(conn, drive, dev, frames: int = 6):

@@ -4,7 +4,6 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <string>
@@ -938,10 +937,6 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         P.pushed_until = h->pushed_until;
         P.epoch = h->epoch;
         P.barrier_cycles = h->barrier_cycles;
-        {
-            const char* gv = std::getenv("FLYBRAIN_PUSH_GATE");   // A/B of the push gate (temporary)
-            P.push_gate = gv ? std::atoi(gv) : 1;
-        }
         CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
         int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
                                    record, h->lanes, st);

@@ -71,7 +71,6 @@ struct PersistArgs {
     int64_t pushed_until;     // the arrivals of every tick < pushed_until are in the accumulators
     int32_t epoch;            // K: steps between grid barriers (2K accumulator slots, 2K + 1 <= n_delay)
     long long barrier_cycles; // the grid barrier's wait budget (SM clock cycles) before it times out
-    int32_t push_gate;        // 1: the push warps hold their reductions while the neuron loop runs
 };
 
 // Phase stamps (per step and CTA; SM clock cycles, compare within a CTA), in step order: 0 step
@@ -172,8 +171,7 @@ __device__ __forceinline__ bool stage_wait(uint64_t* bar, uint32_t parity, const
 
 // Shared-memory layout of one CTA (bytes), for `per` pairs and accumulator type of `acc_bytes`.
 struct PersistSmem {
-    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, special, kick, hseed, gate, total,
-        words_per_map;
+    int64_t mbar, zero, acc, v, g, kbits, ref, misc, scan, pre, spk, ticks, items, special, kick, total, words_per_map;
     __host__ __device__ PersistSmem(int64_t per, int acc_bytes)
     {
         words_per_map = (per + 4 * PT) / 32 + 1;
@@ -194,9 +192,7 @@ struct PersistSmem {
                                             // deltas and kicks of their neurons; biases, posts, pair, instance
         kick = special + MAX_SPECIAL * (2 * 4 * (8 + 8 + 1) + 4 * 4 + 4 * 4 + 4 + 4);   // kick thresholds of
                                                                                        // 2 x U_THREADS inputs
-        hseed = kick + 2 * U_THREADS * 4;   // per step parity and instance: the inner hashes of the kicks
-        gate = hseed + 2 * 64 * 4;          // neuron warps inside the loop (the push warps' gate)
-        total = gate + 16;
+        total = kick + 2 * U_THREADS * 4;
     }
 };
 
@@ -313,35 +309,23 @@ __device__ __forceinline__ int32_t kick_threshold(float p)
 
 // The Poisson kicks of a U thread's first two input pairs, held for the launch (the probabilities
 // are constant during a launch): the pair and instance {local pair | instance << 18} in registers,
-// the thresholds in shared memory; one hash per pair and step, its per-(step, instance) part
-// mix32(step_no * phi ^ mix32(seed + b)) taken from `hs` (computed once per step and instance).
-__device__ __forceinline__ void kicks_held(const DevNet& N, const int32_t (&kx)[2], const int32_t* s_kt, int tid,
-                                           uint32_t* map, int64_t t, const uint32_t* hs, int32_t b0, int64_t lo,
+// the thresholds in shared memory; one hash per pair and step.
+__device__ __forceinline__ void kicks_held(const DevNet& N, const DevState& S, const int32_t (&kx)[2], const int32_t* s_kt,
+                                           int tid, uint32_t* map, int64_t t, uint32_t step_no, int32_t b0, int64_t lo,
                                            const int64_t* stop)
 {
+    const uint32_t sm = step_no * 0x9e3779b9u;
 #pragma unroll
     for (int u = 0; u < 2; u++) {
         const int32_t thr = s_kt[u * U_THREADS + tid];
         if (thr <= 0) continue;
         const int32_t k = kx[u] & 0x3ffff, bl = kx[u] >> 18;
         if (t >= stop[bl]) continue;
+        const int32_t b = b0 + bl;
         const int32_t i = (int32_t)(lo + k - (int64_t)bl * N.n_pad);
-        const uint32_t h = mix32((uint32_t)((int64_t)(b0 + bl) * N.n + i) ^ hs[bl]);
+        const uint32_t h = mix32((uint32_t)((int64_t)b * N.n + i) ^ mix32(sm ^ mix32(S.seed + (uint32_t)b)));
         if ((int32_t)(h >> 8) < thr) atomicOr(map + (k >> 5), 1u << (k & 31));
     }
-}
-
-// the per-(step, instance) part of the kick hash of step step_no for instance b
-__device__ __forceinline__ uint32_t kick_seed(uint32_t seed, uint32_t step_no, int32_t b)
-{
-    return mix32(step_no * 0x9e3779b9u ^ mix32(seed + (uint32_t)b));
-}
-
-// The push warps' gate: while neuron warps are inside the neuron loop (counter > 0) the reductions
-// wait (bounded), since issued beside the loop they slow it and run at half rate themselves.
-__device__ __forceinline__ void gate_wait(const int32_t* gate)
-{
-    for (int spin = 0; spin < 4096 && *reinterpret_cast<const volatile int32_t*>(gate) > 0; spin++) __nanosleep(64);
 }
 
 // Exclusive prefix of `x` over the threads tid0 = 0..stride-1 (whole warps) and the total; uses
@@ -484,7 +468,7 @@ __device__ __forceinline__ void push_arrivals(const DevNet& N, const DevState& S
 template <typename AccT, int LANES>
 __device__ __forceinline__ void push_epoch(const DevNet& N, const DevState& S, int32_t q, int32_t b0, int64_t a0,
                                            int64_t a1, int32_t* s_pre, int32_t* s_cnt, int32_t* scratch, int4* recs,
-                                           const int64_t* s_reset, const int64_t* s_stop, int ptid, const int32_t* gate)
+                                           const int64_t* s_reset, const int64_t* s_stop, int ptid)
 {
     const int nl = (int)(a1 - a0);
     const int warp = ptid >> 5;
@@ -563,7 +547,6 @@ __device__ __forceinline__ void push_epoch(const DevNet& N, const DevState& S, i
             rb = locate(gb);
             eb.load(N, (int64_t)(uint32_t)rb.x + 8 * (int64_t)(gb - rb.w));
         }
-        if (gate) gate_wait(gate);               // the loads are in flight meanwhile
         AccT* ta = target(ra);
 #pragma unroll
         for (int u = 0; u < 8; u++)
@@ -690,9 +673,6 @@ __global__ void __launch_bounds__(PT, 1)
     // than 2 x U_THREADS, are drawn from the table every step)
     int32_t kx[2] = {0, 0};
     int32_t* s_kt = reinterpret_cast<int32_t*>(smem + lay.kick);
-    uint32_t* s_hs = reinterpret_cast<uint32_t*>(smem + lay.hseed);   // [step parity][instance]
-    int32_t* s_gate = reinterpret_cast<int32_t*>(smem + lay.gate);
-    const int32_t* push_gate = A.push_gate ? s_gate : nullptr;
     if (!RASTER && tid < U_THREADS) {
 #pragma unroll
         for (int u = 0; u < 2; u++) {
@@ -710,8 +690,6 @@ __global__ void __launch_bounds__(PT, 1)
         }
     }
     if (A.steps > 0) kicks_into<RASTER>(N, S, A, maps, 0, A.t0, A.step0, b0, G, lo, e0, e1, tid, PT, s_stop);
-    if (tid < G) s_hs[64 + tid] = kick_seed(S.seed, A.step0 + 1u, b0 + tid);   // step 1 (drawn at step 0)
-    if (tid == 0) *s_gate = 0;
     __syncthreads();
 
     unsigned int barriers = 0;
@@ -771,7 +749,7 @@ __global__ void __launch_bounds__(PT, 1)
             if (ptid == 0) stamp(A, ep0, 7);
             if (pa0 < pa1)
                 push_epoch<AccT, LANES>(N, S, q, b0, pa0, pa1, s_pre, s_cnt, s_scan + 16, s_items, s_reset, s_stop,
-                                        ptid, push_gate);
+                                        ptid);
             if (ptid == 0) stamp(A, ep0, 10);
         } else {
             for (int32_t s = ep0; s < ep1; s++) {
@@ -807,7 +785,7 @@ __global__ void __launch_bounds__(PT, 1)
                             kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0, e1, tid, U_THREADS,
                                                s_stop);
                         } else {
-                            kicks_held(N, kx, s_kt, tid, mnext, t + 1, s_hs + ((s + 1) & 1) * 64, b0, lo, s_stop);
+                            kicks_held(N, S, kx, s_kt, tid, mnext, t + 1, step_no + 1u, b0, lo, s_stop);
                             if (e1 - e0 > 2 * U_THREADS)
                                 kicks_into<RASTER>(N, S, A, mnext, s + 1, t + 1, step_no + 1u, b0, G, lo, e0 + 2 * U_THREADS,
                                                    e1, tid, U_THREADS, s_stop);
@@ -836,7 +814,6 @@ __global__ void __launch_bounds__(PT, 1)
                 if (ok && tid < 4 * n_sp)             // the staged neurons' accumulator values of this step
                     s_sp_acc[(s & 1) * 4 * MAX_SPECIAL + tid] = (int64_t)sacc[s_sp_k[tid >> 2] + (tid & 3)];
                 if (ok) {
-                    if (lane == 0) atomicAdd(s_gate, 1);        // this warp is in the loop: reductions wait
                     int32_t i = i0, bl = bl0;
                     const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
                     for (int32_t kb = 0; kb < cnt; kb += 4 * U_THREADS) {
@@ -887,8 +864,6 @@ __global__ void __launch_bounds__(PT, 1)
                         i += 4 * U_THREADS;
                         while (i >= np) { i -= np; bl++; }
                     }
-                    __syncwarp();
-                    if (lane == 0) atomicSub(s_gate, 1);
                     // the staged neurons' plastic deltas of this step, for the listing warps
                     if (tid < 4 * n_sp) {
                         s_sp_pl[(s & 1) * 4 * MAX_SPECIAL + tid] = sp_pl;
@@ -906,10 +881,8 @@ __global__ void __launch_bounds__(PT, 1)
                     }
                     if (tid == 0) stamp(A, s, 3);
                 } else {
-                    // ---- the kick seeds of step s + 2 (the neuron warps draw that step's kicks at the
-                    //      start of step s + 1, after the step boundary); then the previous step's staged
-                    //      neurons and its spikes: counts, plastic rows, work items ----------------------
-                    if (lt < G) s_hs[(s & 1) * 64 + lt] = kick_seed(S.seed, step_no + 2u, b0 + lt);
+                    // ---- the previous step's staged neurons, then its spikes: counts, plastic rows,
+                    //      work items --------------------------------------------------------------
                     if (s >= 1 && n_sp > 0) {
                         if (lt < 4 * n_sp) advance_staged(s - 1, t - 1, lt);
                         list_sync();
