@@ -317,8 +317,49 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tc(const uint16_t* __restri
 // tensor-core MMAs from swizzled K-major descriptors as each stage lands and releases the stage with
 // tcgen05.commit; all four warps then read the accumulator from TMEM for the epilogue. No cluster
 // multicast anywhere. Every wait is bounded; after a timeout no result is written.
+//
+// Split K (gridDim.z = S > 1, launched as clusters of 1 x 1 x S blocks): block z of a cluster
+// accumulates K tiles [z * nk / S, (z + 1) * nk / S) of the same output tile, writes its FP32
+// partial to its own shared memory (the drained stage ring), and after a cluster barrier each block
+// sums its 1/S share of the tile's elements over the S partials in the order z = 0 .. S-1 through
+// distributed shared memory (ld.shared::cluster), then applies the epilogue with consecutive
+// threads on consecutive columns. The sum order is fixed, so a result depends on S and never on
+// scheduling. A second cluster barrier keeps every block's shared memory alive until all reads end.
 // ---------------------------------------------------------------------------------------------
 constexpr int TMA_STAGES = 4;
+constexpr int MAX_SPLIT = 8;                 // portable cluster size
+
+// generic-proxy accesses of shared memory after (or before) the tensor-core / TMA proxy's
+__device__ __forceinline__ void fence_async_to_generic() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ uint32_t cluster_rank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// the shared-memory address `local` of this block, as seen in block `rank` of the cluster
+__device__ __forceinline__ uint32_t map_rank(uint32_t local, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ float ld_cluster_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(addr) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_cluster_s32(uint32_t addr)
+{
+    int v;
+    asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+    return v;
+}
 
 // shared-memory descriptor, K-major with the 128-byte swizzle: 8-row atoms of 1024 bytes (SBO), the
 // K offset inside the 128-byte row added to the start address (LBO unused: 16 bytes)
@@ -373,7 +414,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tma(const __grid_constant__
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = s_tmem;
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
-    const int nk = (K + 63) / 64;
+    // this block's K tiles: all of them, or its share of a split (every share has at least one)
+    const int S = (int)gridDim.z, z = S > 1 ? (int)cluster_rank() : 0;
+    const int nk_all = (K + 63) / 64, kt0 = (int)((int64_t)z * nk_all / S);
+    const int nk = (int)((int64_t)(z + 1) * nk_all / S) - kt0;
     if (tid == 0) {                                   // producer: the TMA loads
         int kt = 0;
         for (; kt < nk; kt++) {
@@ -385,8 +429,8 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tma(const __grid_constant__
             const uint32_t sa = base + s * STAGE;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(&full[s])), "r"(STAGE)
                          : "memory");
-            tma_load_2d(sa, &mapA, kt * 64, m0, su32(&full[s]));
-            tma_load_2d(sa + A_BYTES, &mapB, kt * 64, n0, su32(&full[s]));
+            tma_load_2d(sa, &mapA, (kt0 + kt) * 64, m0, su32(&full[s]));
+            tma_load_2d(sa + A_BYTES, &mapB, (kt0 + kt) * 64, n0, su32(&full[s]));
         }
         s_issued = kt;
     } else if (tid == 32) {                           // the MMA issuer
@@ -420,10 +464,17 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tma(const __grid_constant__
                      : "memory");
     }
     const bool fin = tc_wait(su32(&done), 0u);
+    // loads still in flight after a timeout land before the stage ring is reused or the block
+    // leaves (bounded)
+    if (tid == 0)
+        for (int kt = s_used; kt < s_issued; kt++) (void)tc_wait(su32(&full[kt % TMA_STAGES]), (uint32_t)((kt / TMA_STAGES) & 1));
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     __syncthreads();
     const bool ok = fin && s_ok != 0;
     const int row = m0 + warp * 32 + lane;
+    constexpr int PSTR = BN + 1;                      // partial rows padded: a warp's 32 rows hit 32 banks
+    float* part = reinterpret_cast<float*>(dyn + (base - su32(dyn)));
+    if (S > 1) fence_async_to_generic();
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 16) {
         uint32_t v[16];
@@ -434,14 +485,31 @@ __global__ void __launch_bounds__(TC_THREADS) k_gemm_tma(const __grid_constant__
               "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
             : "r"(addr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (ok) {
+        if (S > 1) {
+#pragma unroll
+            for (int j = 0; j < 16; j++) part[(warp * 32 + lane) * PSTR + c0 + j] = __uint_as_float(v[j]);
+        } else if (ok) {
 #pragma unroll
             for (int j = 0; j < 16; j++) epilogue(e, M, N, row, n0 + c0 + j, __uint_as_float(v[j]));
         }
     }
-    // loads still in flight after a timeout land before the block leaves (bounded)
-    if (tid == 0)
-        for (int kt = s_used; kt < s_issued; kt++) (void)tc_wait(su32(&full[kt % TMA_STAGES]), (uint32_t)((kt / TMA_STAGES) & 1));
+    if (S > 1) {
+        if (tid == 0) s_ok = ok ? 1 : 0;
+        cluster_sync_all();                           // every partial is written and visible
+        bool all_ok = true;
+        for (int r = 0; r < S; r++) all_ok = all_ok && ld_cluster_s32(map_rank(su32(&s_ok), (uint32_t)r)) != 0;
+        constexpr int TILE = TC_BM * BN;
+        const int chunk = (TILE + S - 1) / S, lo = z * chunk, hi = min(TILE, lo + chunk);
+        const uint32_t pbase = su32(part);
+        for (int el = lo + tid; el < hi; el += TC_THREADS) {
+            const int r = el / BN, c = el - r * BN;
+            const uint32_t off = (uint32_t)(r * PSTR + c) * 4u;
+            float acc = 0.0f;
+            for (int q = 0; q < S; q++) acc += ld_cluster_f32(map_rank(pbase + off, (uint32_t)q));
+            if (all_ok) epilogue(e, M, N, m0 + r, n0 + c, acc);
+        }
+        cluster_sync_all();                           // no block leaves while another reads its partial
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
@@ -472,44 +540,109 @@ __global__ void k_poisson(const float* z, const float* y, int M, int D, double* 
     }
 }
 
-__global__ void k_colsum(const uint16_t* X, int M, int N, int ld, float* grad)
+// column sums: a cluster of S blocks per 32 columns, block z of it over rows [z M / S, (z + 1) M / S)
+// with its 32 warps on interleaved rows (lanes on consecutive columns); the warps' partials, then
+// the blocks' (through distributed shared memory), added in a fixed order
+__global__ void __launch_bounds__(1024) k_colsum(const uint16_t* X, int M, int N, int ld, float* grad)
 {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N) return;
+    __shared__ float part[32][33];
+    __shared__ float tot[32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, j = blockIdx.x * 32 + lane;
+    const int S = (int)gridDim.y, z = S > 1 ? (int)cluster_rank() : 0;
+    const int r0 = (int)((int64_t)z * M / S), r1 = (int)((int64_t)(z + 1) * M / S);
     float s = 0.0f;
-    for (int i = 0; i < M; i++) s += __bfloat162float(__ushort_as_bfloat16(X[(int64_t)i * ld + j]));
-    grad[j] = s;
+    if (j < N) {
+#pragma unroll 8
+        for (int i = r0 + w; i < r1; i += 32) s += __bfloat162float(__ushort_as_bfloat16(X[(int64_t)i * ld + j]));
+    }
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0) {
+        float t = 0.0f;
+        for (int q = 0; q < 32; q++) t += part[q][lane];
+        tot[lane] = t;
+    }
+    if (S > 1) cluster_sync_all();
+    else __syncthreads();
+    if (z == 0 && w == 0 && j < N) {
+        float t = 0.0f;
+        for (int q = 0; q < S; q++) t += S > 1 ? ld_cluster_f32(map_rank(su32(&tot[lane]), (uint32_t)q)) : tot[lane];
+        grad[j] = t;
+    }
+    if (S > 1) cluster_sync_all();                    // no block leaves while block 0 reads its sums
+}
+
+// Adam on one element; returns the new weight
+__device__ __forceinline__ float adam_one(float* w, const float* g, float* m, float* v, int64_t p, float lr, float b1,
+                                          float b2, float eps, float c1, float c2)
+{
+    const float gg = g[p];
+    const float mm = b1 * m[p] + (1.0f - b1) * gg;
+    const float vv = b2 * v[p] + (1.0f - b2) * gg * gg;
+    m[p] = mm;
+    v[p] = vv;
+    const float ww = w[p] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+    w[p] = ww;
+    return ww;
 }
 
 __global__ void k_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr, float b1, float b2, float eps,
-                       float c1, float c2, uint16_t* wb, uint16_t* wbt, int rows, int cols, int ldt)
+                       float c1, float c2, uint16_t* wb)
 {
     for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        const float gg = g[p];
-        const float mm = b1 * m[p] + (1.0f - b1) * gg;
-        const float vv = b2 * v[p] + (1.0f - b2) * gg * gg;
-        m[p] = mm;
-        v[p] = vv;
-        const float ww = w[p] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
-        w[p] = ww;
-        const uint16_t h = f2bf(ww);
+        const uint16_t h = f2bf(adam_one(w, g, m, v, p, lr, b1, b2, eps, c1, c2));
         if (wb) wb[p] = h;
-        if (wbt) {
-            const int64_t r = p / cols, c = p - r * cols;
-            wbt[c * ldt + r] = h;
-        }
     }
 }
 
-__global__ void k_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* out_t, int rows, int cols, int ldt)
+// The same on a rows x cols weight in 32 x 32 tiles (block 32 x 8), with its transposed bf16 copy
+// written through shared memory so that both copies are stored along rows
+__global__ void k_adam_t(float* w, const float* g, float* m, float* v, float lr, float b1, float b2, float eps, float c1,
+                         float c2, uint16_t* wb, uint16_t* wbt, int rows, int cols, int ldt)
 {
-    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
-        const uint16_t h = f2bf(x[p]);
-        if (out) out[p] = h;
-        if (out_t) {
-            const int64_t r = p / cols, c = p - r * cols;
-            out_t[c * ldt + r] = h;
+    __shared__ uint16_t tile[32][34];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32, tx = threadIdx.x, ty = threadIdx.y;
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + tx;
+        if (r < rows && c < cols) {
+            const int64_t p = (int64_t)r * cols + c;
+            const uint16_t h = f2bf(adam_one(w, g, m, v, p, lr, b1, b2, eps, c1, c2));
+            if (wb) wb[p] = h;
+            tile[k][tx] = h;
         }
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + tx;
+        if (r < rows && c < cols) wbt[(int64_t)c * ldt + r] = tile[tx][k];
+    }
+}
+
+__global__ void k_to_bf16(const float* x, int64_t n, uint16_t* out)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        out[p] = f2bf(x[p]);
+}
+
+// FP32 -> bf16 of a rows x cols matrix in 32 x 32 tiles (block 32 x 8): the plain copy (when `out`)
+// and the transposed one, both stored along rows
+__global__ void k_to_bf16_t(const float* x, uint16_t* out, uint16_t* out_t, int rows, int cols, int ldt)
+{
+    __shared__ uint16_t tile[32][34];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32, tx = threadIdx.x, ty = threadIdx.y;
+    for (int k = ty; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + tx;
+        if (r < rows && c < cols) {
+            const int64_t p = (int64_t)r * cols + c;
+            const uint16_t h = f2bf(x[p]);
+            if (out) out[p] = h;
+            tile[k][tx] = h;
+        }
+    }
+    __syncthreads();
+    for (int k = ty; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + tx;
+        if (r < rows && c < cols) out_t[(int64_t)c * ldt + r] = tile[tx][k];
     }
 }
 
@@ -568,6 +701,23 @@ bool tensor_map(CUtensorMap* map, const uint16_t* X, int rows, int K, int ld, in
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+int g_gemm_split = MAX_SPLIT;
+
+// K split of a TMA GEMM: enough blocks to fill the SMs at `per_sm` blocks each (the kernel's
+// shared-memory occupancy), at least eight 64-deep K tiles per block (below that the cluster
+// reduction costs more than the split saves), at most the set limit
+int split_for(int tiles, int K, int per_sm)
+{
+    if (g_gemm_split <= 1) return 1;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        sms = 148;
+    }
+    const int nk = (K + 63) / 64;
+    return std::max(1, std::min({g_gemm_split, (per_sm * sms) / std::max(tiles, 1), nk / 8}));
+}
+
 // 1: launched; 0: not eligible for TMA (the caller falls back); negative: an error code
 template <int BN>
 int launch_tma(const uint16_t* A, const uint16_t* B, int M, int N, int K, int lda, int ldb, const Epi& e, cudaStream_t st)
@@ -575,14 +725,32 @@ int launch_tma(const uint16_t* A, const uint16_t* B, int M, int N, int K, int ld
     CUtensorMap ma, mb;
     if (!tensor_map(&ma, A, M, K, lda, TC_BM) || !tensor_map(&mb, B, N, K, ldb, BN)) return 0;
     constexpr int smem = TMA_STAGES * (TC_BM * 128 + BN * 128) + 1024;
+    static_assert(TC_BM * (BN + 1) * 4 <= TMA_STAGES * (TC_BM * 128 + BN * 128), "split-K partials fit the stage ring");
     static bool attr = false;
     if (!attr) {
         if (cudaFuncSetAttribute(k_gemm_tma<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
             return -cuda_status();
         attr = true;
     }
-    dim3 grid((N + BN - 1) / BN, (M + TC_BM - 1) / TC_BM);
-    k_gemm_tma<BN><<<grid, TC_THREADS, smem, st>>>(ma, mb, M, N, K, e);
+    const unsigned gx = (N + BN - 1) / BN, gy = (M + TC_BM - 1) / TC_BM;
+    const int S = split_for((int)(gx * gy), K, smem * 2 <= 227 * 1024 ? 2 : 1);
+    if (S == 1) {
+        k_gemm_tma<BN><<<dim3(gx, gy), TC_THREADS, smem, st>>>(ma, mb, M, N, K, e);
+    } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(gx, gy, (unsigned)S);
+        cfg.blockDim = dim3(TC_THREADS);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 1;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = (unsigned)S;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        if (cudaLaunchKernelEx(&cfg, k_gemm_tma<BN>, ma, mb, M, N, K, e) != cudaSuccess) return -cuda_status();
+    }
     const int rc = cuda_status();
     return rc == FB_OK ? 1 : -rc;
 }
@@ -627,6 +795,14 @@ extern "C" int fs_gemm_kind(int32_t kind)
     return old;
 }
 
+extern "C" int fs_gemm_split(int32_t max_split)
+{
+    if (max_split == 0 || max_split < -1 || max_split > MAX_SPLIT) return -fail("fs_gemm_split: 1 .. 8, or -1 to keep");
+    const int old = g_gemm_split;
+    if (max_split > 0) g_gemm_split = max_split;
+    return old;
+}
+
 extern "C" int fs_poisson_nll(const float* z, const float* y, int32_t M, int32_t D, double* loss_sum, uint16_t* dz,
                               int32_t ldd, uint16_t* dz_t, void* stream)
 {
@@ -638,7 +814,23 @@ extern "C" int fs_poisson_nll(const float* z, const float* y, int32_t M, int32_t
 extern "C" int fs_colsum(const uint16_t* X, int32_t M, int32_t N, int32_t ld, float* grad, void* stream)
 {
     if (!X || !grad || M <= 0 || N <= 0 || ld < N) return fail("fs_colsum: bad arguments");
-    k_colsum<<<(N + 127) / 128, 128, 0, (cudaStream_t)stream>>>(X, M, N, ld, grad);
+    const int S = std::min(MAX_SPLIT, std::max(1, M / 256));    // >= 8 rows per warp
+    if (S == 1) {
+        k_colsum<<<(N + 31) / 32, 1024, 0, (cudaStream_t)stream>>>(X, M, N, ld, grad);
+        return cuda_status();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((N + 31) / 32), (unsigned)S);
+    cfg.blockDim = dim3(1024);
+    cfg.stream = (cudaStream_t)stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 1;
+    at[0].val.clusterDim.y = (unsigned)S;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    if (cudaLaunchKernelEx(&cfg, k_colsum, X, M, N, ld, grad) != cudaSuccess) return cuda_status();
     return cuda_status();
 }
 
@@ -647,11 +839,16 @@ extern "C" int fs_adam(float* w, const float* grad, float* m, float* v, int64_t 
                        int32_t ldt, void* stream)
 {
     if (!w || !grad || !m || !v || n <= 0 || t < 1) return fail("fs_adam: bad arguments");
-    if (w_bf16_t && ((int64_t)rows * cols != n || ldt < rows))
-        return fail("fs_adam: the transposed copy needs rows * cols == n and ldt >= rows");
+    if (w_bf16_t && (rows <= 0 || cols <= 0 || rows > 65535 * 32 || (int64_t)rows * cols != n || ldt < rows))
+        return fail("fs_adam: the transposed copy needs 0 < rows <= 2097120, rows * cols == n and ldt >= rows");
     const float c1 = 1.0f - powf(beta1, (float)t), c2 = 1.0f - powf(beta2, (float)t);
-    k_adam<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(w, grad, m, v, n, lr, beta1, beta2, eps, c1, c2, w_bf16,
-                                                            w_bf16_t, rows, cols, ldt);
+    if (w_bf16_t) {
+        const dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+        k_adam_t<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(w, grad, m, v, lr, beta1, beta2, eps, c1, c2, w_bf16,
+                                                                 w_bf16_t, rows, cols, ldt);
+    } else {
+        k_adam<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(w, grad, m, v, n, lr, beta1, beta2, eps, c1, c2, w_bf16);
+    }
     return cuda_status();
 }
 
@@ -659,8 +856,13 @@ extern "C" int fs_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* ou
                           int32_t ldt, void* stream)
 {
     if (!x || n <= 0 || (!out && !out_t)) return fail("fs_to_bf16: bad arguments");
-    if (out_t && ((int64_t)rows * cols != n || ldt < rows))
-        return fail("fs_to_bf16: the transposed copy needs rows * cols == n and ldt >= rows");
-    k_to_bf16<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(x, n, out, out_t, rows, cols, ldt);
+    if (out_t && (rows <= 0 || cols <= 0 || rows > 65535 * 32 || (int64_t)rows * cols != n || ldt < rows))
+        return fail("fs_to_bf16: the transposed copy needs 0 < rows <= 2097120, rows * cols == n and ldt >= rows");
+    if (out_t) {
+        const dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+        k_to_bf16_t<<<grid, dim3(32, 8), 0, (cudaStream_t)stream>>>(x, out, out_t, rows, cols, ldt);
+    } else {
+        k_to_bf16<<<blocks_for(n), 256, 0, (cudaStream_t)stream>>>(x, n, out);
+    }
     return cuda_status();
 }

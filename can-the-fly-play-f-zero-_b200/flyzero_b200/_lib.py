@@ -85,6 +85,7 @@ SIGNATURES = {
                                 C.c_uint32, C.c_int64, C.c_int32, C.c_int32, vp, vp]),
     # include/flysurrogate.h
     "fs_gemm_kind": (C.c_int, [C.c_int32]),
+    "fs_gemm_split": (C.c_int, [C.c_int32]),
     "fs_gemm": (C.c_int, [vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp,
                           vp, C.c_int32, C.c_int32, vp]),
     "fs_poisson_nll": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32, vp, vp]),

@@ -177,3 +177,58 @@ class MLP:
         import torch
 
         return torch.exp(self.forward(X))
+
+
+GEMM_SHAPES = ((4096, 512, 1280), (4096, 512, 512), (4096, 10, 512),      # forward, batch 4096
+               (512, 1280, 4096), (512, 512, 4096), (10, 512, 4096),      # weight gradients
+               (4096, 512, 512), (4096, 512, 16))                         # input gradients
+
+
+def time_kernels(batch: int = 4096, reps: int = 50, warm: int = 5) -> dict:
+    """Device times (CUDA events on the current stream, `reps` launches after `warm`) of fs_gemm on the
+    training step's shapes (F32 epilogue, TMA kind) with and without the K split, and of a whole
+    training step at `batch`. Returns {name: microseconds}."""
+    import torch
+
+    L = _lib.load()
+    old_kind, old_split = L.fs_gemm_kind(2), L.fs_gemm_split(-1)
+    st = _stream(torch.cuda.current_device())
+
+    def timed(fn):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps * 1e3
+
+    out = {}
+    g = torch.Generator(device="cuda").manual_seed(0)
+    try:
+        for M, N, K in GEMM_SHAPES:
+            A = torch.randn((M, K), device="cuda", generator=g).to(torch.bfloat16)
+            B = torch.randn((N, K), device="cuda", generator=g).to(torch.bfloat16)
+            C_ = torch.empty((M, N), device="cuda")
+            for split in (1, old_split):
+                L.fs_gemm_split(split)
+                out[f"gemm {M}x{N}x{K} split<={split}"] = timed(lambda: _lib.check(
+                    L.fs_gemm(_p(A), _p(B), M, N, K, K, K, 0, None, None, _p(C_), None, None, N, 0, st)))
+        L.fs_gemm_split(old_split)
+        net = MLP(seed=0)
+        X = torch.randn((batch, DIMS[0]), device="cuda", generator=g)
+        Y = torch.poisson(torch.ones((batch, DIMS[-1]), device="cuda"), generator=g)
+        out[f"train_step batch={batch}"] = timed(lambda: net.train_step(X, Y))
+    finally:
+        L.fs_gemm_kind(old_kind)
+        L.fs_gemm_split(old_split)
+    return out
+
+
+if __name__ == "__main__":
+    import json
+
+    print(json.dumps({k: round(v, 2) for k, v in time_kernels().items()}, indent=1))

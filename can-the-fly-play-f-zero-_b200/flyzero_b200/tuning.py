@@ -206,8 +206,11 @@ def train(net, X, Y, epochs: int, batch: int = 4096, seed: int = 0):
     return losses
 
 
-def surrogate_episode(net, feat, xy, x, frames: int):
-    """Predicted expected DN counts (N, frames, 10) of candidates x (N, 12) (torch on the GPU)."""
+def surrogate_episode(net, feat, xy, x, frames: int, cap=None):
+    """Predicted expected DN counts (N, frames, 10) of candidates x (N, 12) (torch on the GPU). The
+    rollout feeds each frame's prediction back as the next frame's previous counts; `cap` (10,),
+    the largest count of each DN in the simulated frames, bounds what is fed back and predicted, so
+    that an overrated frame cannot run away outside the range the network was trained on."""
     import torch
 
     xs = torch.as_tensor(np.asarray(x, np.float32), device=feat.device)
@@ -216,6 +219,8 @@ def surrogate_episode(net, feat, xy, x, frames: int):
     for f in range(frames):
         X = feat(interface_rates(xs, xy, f * wl.FRAME_MS), prev)
         mu = torch.exp(net.forward(X).clamp(-20.0, 8.0))      # bounded: predictions feed back
+        if cap is not None:
+            mu = torch.minimum(mu, cap)
         out[:, f] = mu
         prev = mu
     return out
@@ -254,9 +259,10 @@ def search_with_surrogate(net, feat, sim, generations: int, popsize: int = 1024,
     g_rng = torch.Generator(device=feat.device).manual_seed(seed)
     newX, newY = [], []
     scale = np.ones(10)                          # per-DN calibration of the predicted counts
+    cap = data[1].amax(0).float() if data is not None else None
     for g in range(generations):
         X = es.ask()
-        raw = surrogate_episode(net, feat, sim.xy, X, frames).cpu().numpy()
+        raw = surrogate_episode(net, feat, sim.xy, X, frames, cap).cpu().numpy()
         pc = raw * scale
         pf = fitness(pc)
         top = np.argsort(-pf, kind="stable")[:survivors]
@@ -268,6 +274,7 @@ def search_with_surrogate(net, feat, sim, generations: int, popsize: int = 1024,
         per = float(np.mean(count_error(pc[top], tc)))
         newX.append(tfeat.reshape(-1, 1280))
         newY.append(tc_d.reshape(-1, 10))
+        cap = newY[-1].amax(0).float() if cap is None else torch.maximum(cap, newY[-1].amax(0).float())
         if refine_steps and data is not None:
             NX, NY = torch.cat(newX), torch.cat(newY)
             for _ in range(refine_steps):
@@ -276,9 +283,9 @@ def search_with_surrogate(net, feat, sim, generations: int, popsize: int = 1024,
                 net.train_step(torch.cat([NX[i_new], data[0][i_old]]).contiguous(),
                                torch.cat([NY[i_new], data[1][i_old]]).contiguous())
         # calibration for the next generation: the refined network on these survivors
-        again = surrogate_episode(net, feat, sim.xy, X[top], frames).cpu().numpy()
+        again = surrogate_episode(net, feat, sim.xy, X[top], frames, cap).cpu().numpy()
         scale = tc.sum((0, 1)) / np.maximum(again.sum((0, 1)), 1e-6)
-        scale = np.where(tc.sum((0, 1)) > 0, scale, 1.0)
+        scale = np.clip(np.where(tc.sum((0, 1)) > 0, scale, 1.0), 0.25, 4.0)   # a DN predicted silent: bounded
         if err <= tol:
             f_all = pf.copy()
             f_all[top] = tf

@@ -28,7 +28,7 @@ extern "C" {
 
 /* GEMM kinds: the BF16 m16n8k16 warp MMA; tcgen05 (one thread issues 128 x N x 16 tensor-core
  * MMAs from shared-memory descriptors, FP32 accumulator in tensor memory) with operands staged by
- * cp.async; or the same fed by TMA (2-D tensor loads with the 128-byte swizzle into a 6-stage
+ * cp.async; or the same fed by TMA (2-D tensor loads with the 128-byte swizzle into a 4-stage
  * mbarrier ring; operands whose base is not 16-byte aligned take the cp.async form). Default: TMA. */
 #define FS_GEMM_MMA_SYNC 0
 #define FS_GEMM_TCGEN05 1
@@ -36,6 +36,14 @@ extern "C" {
 
 /* Select the kind fs_gemm uses (-1: keep); returns the previous kind. */
 int fs_gemm_kind(int32_t kind);
+
+/* Largest K split of the TMA kind (1 .. 8; -1: keep; default 8); returns the previous limit. A GEMM
+ * with few output tiles and a long K (the weight gradients: M = 512, K = the batch) splits each
+ * tile's K range over a cluster of up to that many blocks, enough to fill two blocks per SM with at
+ * least four 64-deep K tiles each; the FP32 partials are summed in a fixed order, so results
+ * depend on the split chosen for the shape and limit, not on scheduling. A bad limit returns
+ * -FB_ERR_ARG. */
+int fs_gemm_split(int32_t max_split);
 
 /* C[M x N] = A[M x K] * B[N x K]^T with bf16 A (row stride lda), bf16 B (row stride ldb), FP32
  * accumulation, then the epilogue `epi` writing rows of stride ldo (transposed outputs: stride
@@ -55,13 +63,13 @@ int fs_colsum(const uint16_t* X, int32_t M, int32_t N, int32_t ld, float* grad, 
 
 /* Adam on FP32 master weights w[n] with FP32 moments m, v: bias-corrected with step t (>= 1);
  * writes the bf16 copy w_bf16 (same layout) and, when w_bf16_t != NULL, the transposed bf16 copy
- * of the rows x cols weight (rows * cols == n) with row stride ldt >= rows. */
+ * of the rows x cols weight (rows * cols == n, 0 < rows <= 2,097,120) with row stride ldt >= rows. */
 int fs_adam(float* w, const float* grad, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
             float eps, int32_t t, uint16_t* w_bf16, uint16_t* w_bf16_t, int32_t rows, int32_t cols, int32_t ldt,
             void* stream);
 
 /* FP32 -> bf16 (round to nearest even); optional transposed copy of the rows x cols matrix
- * (rows * cols == n) with row stride ldt >= rows. */
+ * (rows * cols == n, 0 < rows <= 2,097,120) with row stride ldt >= rows. */
 int fs_to_bf16(const float* x, int64_t n, uint16_t* out, uint16_t* out_t, int32_t rows, int32_t cols, int32_t ldt,
                void* stream);
 
