@@ -629,8 +629,13 @@ extern "C" int fb_reward_step(fb_brain* h, const int32_t* counts, double* elig, 
     a.w0 = h->w0; a.pw = h->pw; a.elig = elig; a.post_mean = post_mean; a.coef = coef;
     a.fly_ptr = fly_ptr; a.fly_slots = fly_slots; a.fly_weight = fly_weight; a.mask = mask;
     a.ae = ae; a.ap = ap; a.cap = cap; a.w_syn = (float)h->params.w_syn; a.apply = apply;
-    k_reward_elig<<<(unsigned)((h->n_pl + 255) / 256), 256, 0, st>>>(a);
+    k_reward_elig<<<(unsigned)(((int64_t)h->B * h->n_pl + 255) / 256), 256, 0, st>>>(a);
     CU(cudaGetLastError());
+    if (apply) {
+        k_reward_apply<<<(unsigned)(((int64_t)n_flies * h->n_pl + 255) / 256), 256, 0, st>>>(a);
+        CU(cudaGetLastError());
+        h->launches += 1;
+    }
     const int64_t np_ = (int64_t)h->B * h->n_ppost;
     k_reward_post_mean<<<(unsigned)((np_ + 255) / 256), 256, 0, st>>>(a);
     CU(cudaGetLastError());

@@ -1,4 +1,5 @@
-// The reward-modulated plastic-synapse rule, fused on the device (one launch per frame each):
+// The reward-modulated plastic-synapse rule on the device (traces, update, running means: three
+// launches per frame):
 //
 //   flyzero/learning.py:116-131 (one instance, RewardPlasticity.step) and flyzero/batch.py:158-172,
 //   482-495 (BatchReward.step with _Plastic.apply; flyzero/school.py:289-304 with per-slot rates):
@@ -39,37 +40,46 @@ struct RewardArgs {
     int32_t apply;
 };
 
+// the traces: one thread per (instance b, plastic entry k), b-major so that a warp's E and
+// counts of one instance are contiguous
 __global__ void __launch_bounds__(256) k_reward_elig(const RewardArgs a)
 {
-    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.n_pl || (a.mask && !a.mask[k])) return;
-    const int32_t pre = a.pre[k], post = a.post[k], q = a.pidx[k];
-    for (int32_t b = 0; b < a.B; b++) {
-        const float c_pre = __int2float_rn(a.counts[(int64_t)b * a.n + pre]);
-        const float c_post = __int2float_rn(a.counts[(int64_t)b * a.n + post]);
-        const float dev = __fsub_rn(c_post, a.post_mean[(int64_t)b * a.n_ppost + q]);
-        double* e = a.elig + (int64_t)b * a.n_pl + k;
-        *e = __dadd_rn(__dmul_rn(a.ae, *e), (double)__fmul_rn(c_pre, dev));
-    }
-    if (!a.apply) return;
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)a.B * a.n_pl) return;
+    const int32_t b = (int32_t)(p / a.n_pl);
+    const int64_t k = p - (int64_t)b * a.n_pl;
+    if (a.mask && !a.mask[k]) return;
+    const float c_pre = __int2float_rn(a.counts[(int64_t)b * a.n + a.pre[k]]);
+    const float c_post = __int2float_rn(a.counts[(int64_t)b * a.n + a.post[k]]);
+    const float dev = __fsub_rn(c_post, a.post_mean[(int64_t)b * a.n_ppost + a.pidx[k]]);
+    double* e = a.elig + p;
+    *e = __dadd_rn(__dmul_rn(a.ae, *e), (double)__fmul_rn(c_pre, dev));
+}
+
+// the per-fly averaged update and the clip: one thread per (fly f, plastic entry k); the fly's
+// slots are summed in slot order
+__global__ void __launch_bounds__(256) k_reward_apply(const RewardArgs a)
+{
+    const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= (int64_t)a.n_flies * a.n_pl) return;
+    const int32_t f = (int32_t)(p / a.n_pl);
+    const int64_t k = p - (int64_t)f * a.n_pl;
+    if (a.mask && !a.mask[k]) return;
     const float w0 = a.w0[k];
     const float sg = w0 > 0.0f ? 1.0f : (w0 < 0.0f ? -1.0f : 0.0f);
     const double wmax = (double)__fmul_rn(a.cap, fmaxf(fabsf(w0), a.w_syn));
     const double sgd = (double)sg;
-    for (int32_t f = 0; f < a.n_flies; f++) {
-        double s = 0.0;
-        for (int32_t j = a.fly_ptr[f]; j < a.fly_ptr[f + 1]; j++) {
-            const int32_t b = a.fly_slots[j];
-            const float wgt = a.fly_weight[b];
-            if (wgt != 0.0f)
-                s = __dadd_rn(s, __dmul_rn((double)wgt, __dmul_rn(a.coef[b], a.elig[(int64_t)b * a.n_pl + k])));
-        }
-        for (int32_t j = a.fly_ptr[f]; j < a.fly_ptr[f + 1]; j++) {
-            const int32_t b = a.fly_slots[j];
-            float* w = a.pw + (int64_t)b * a.n_pl + k;
-            const double x = __dmul_rn(sgd, __dadd_rn((double)*w, s));
-            *w = __double2float_rn(__dmul_rn(sgd, fmin(fmax(x, 0.0), wmax)));
-        }
+    double s = 0.0;
+    for (int32_t j = a.fly_ptr[f]; j < a.fly_ptr[f + 1]; j++) {
+        const int32_t b = a.fly_slots[j];
+        const float wgt = a.fly_weight[b];
+        if (wgt != 0.0f) s = __dadd_rn(s, __dmul_rn((double)wgt, __dmul_rn(a.coef[b], a.elig[(int64_t)b * a.n_pl + k])));
+    }
+    for (int32_t j = a.fly_ptr[f]; j < a.fly_ptr[f + 1]; j++) {
+        const int32_t b = a.fly_slots[j];
+        float* w = a.pw + (int64_t)b * a.n_pl + k;
+        const double x = __dmul_rn(sgd, __dadd_rn((double)*w, s));
+        *w = __double2float_rn(__dmul_rn(sgd, fmin(fmax(x, 0.0), wmax)));
     }
 }
 

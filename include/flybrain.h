@@ -139,7 +139,8 @@ int fb_reset(fb_brain* brain, const int32_t* flies /*[host]*/, int32_t n_flies, 
 int fb_run(fb_brain* brain, int32_t steps, int32_t* counts_out, const uint32_t* kicks,
            int32_t* step_counts, uint64_t* step_digest, void* stream);
 
-/* The reward-modulated plastic update of every instance, fused on the device (two launches).
+/* The reward-modulated plastic update of every instance on the device (traces per instance and
+ * entry, the update per fly and entry, the running means: three launches, two when apply is 0).
  * Restates RewardPlasticity.step (flyzero/learning.py:116-131) for one instance and
  * BatchReward.step + _Plastic.apply (flyzero/batch.py:158-172, 482-495) for many:
  *   E = ae*E + c[pre]*(c[post] - <post>);  per fly f: s_f = sum_{learning b of f} fly_weight[b]*coef[b]*E_b;
@@ -150,7 +151,8 @@ int fb_run(fb_brain* brain, int32_t steps, int32_t* counts_out, const uint32_t* 
  *   post_mean  [device] (batch, n_targets) float32 running mean count of each plastic target
  *              (targets = distinct postsynaptic neurons of the plastic entries, ascending)
  *   coef       [device] (batch) float64: eta * advantage of each slot, rounded as the rule does
- *   fly_ptr    [device] (n_flies+1), fly_slots [device] (batch): slots grouped by fly
+ *   fly_ptr    [device] (n_flies+1), fly_slots [device] (batch): slots grouped by fly, each slot in
+ *              one fly at most (the flies' updates run in parallel)
  *   fly_weight [device] (batch) float32: 1/(learning slots of the fly) for a learning slot, else 0
  *   mask       [device] NULL or (n_plastic) uint8: the plastic entries this rule owns (others untouched)
  *   apply      0: traces and means only (no slot learns this frame, batch.py:493) */
