@@ -23,7 +23,8 @@
 //   push warps (4): per epoch, scatter this CTA's share of the items arriving in the next epoch.
 // Three bitmaps rotate: map[s%3] holds the kicks of step s, then (overwritten by the neuron warps)
 // its spikes; map[(s+1)%3] receives the next kicks; the listing warps read and clear map[(s-1)%3].
-// Every wait is bounded: after ~4 s a CTA raises the timeout flag and every CTA returns.
+// Every wait is bounded: after ~4 s a CTA raises the timeout flag and every CTA returns (the others
+// read the flag in the grid barrier, so within an epoch a CTA waits only on its own bulk loads).
 #pragma once
 #include "engine.cuh"
 
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(PT, 1)
                 ul_sync();                       // neuron and listing warps: step boundary
                 if (is_u) {
                     if (tid == 0) stamp(A, s, 0);
-                    if (tid == 0 && cnt > 0 && !staged && !ld_volatile_i32(A.abort_flag))
+                    if (tid == 0 && cnt > 0 && !staged)
                         issue_slice(acc + acc_base, sacc, acc_bytes, mbar);
                     if (tid < G) s_active[tid] = t < s_stop[tid];
                     // a staged neuron's thread: its kick of this step (the loop below overwrites the
@@ -798,7 +799,7 @@ __global__ void __launch_bounds__(PT, 1)
                     if (tid == 0) stamp(A, s, 1);
                     bool ok = true;
                     if (cnt > 0 && tid == 0)
-                        ok = !ld_volatile_i32(A.abort_flag) && stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
+                        ok = stage_wait(mbar, (uint32_t)(s & 1), A, err, s + 1);
                     ok = !u_sync_or(!ok);        // one thread waited; every U thread agrees on the outcome
                     if (cnt > 0 && ok) (void)mbar_try_wait(mbar, (uint32_t)(s & 1));   // completed: acquire only
                     if (tid == 0) stamp(A, s, 2);
