@@ -803,11 +803,14 @@ __global__ void __launch_bounds__(PT, 1)
                     ok = !u_sync_or(!ok);        // one thread waited; every U thread agrees on the outcome
                     if (cnt > 0 && ok) (void)mbar_try_wait(mbar, (uint32_t)(s & 1));   // completed: acquire only
                     if (tid == 0) stamp(A, s, 2);
-                    if (cnt > 0 && ok && tid == 0) {     // the slice is in shared memory: clear it in global memory
-                        AccT* accw = const_cast<AccT*>(acc) + acc_base;
-                        for (uint32_t off = 0; off < acc_bytes; off += ZERO_PAGE)
+                    if (cnt > 0 && ok && tid < 32) {     // the slice is in shared memory: clear it in global
+                        AccT* accw = const_cast<AccT*>(acc) + acc_base;   // memory, a zero page per lane of warp 0
+                        bool any = false;
+                        for (uint32_t off = (uint32_t)tid * ZERO_PAGE; off < acc_bytes; off += 32u * ZERO_PAGE) {
                             tma_store_1d(reinterpret_cast<uint8_t*>(accw) + off, zero, min((uint32_t)ZERO_PAGE, acc_bytes - off));
-                        bulk_commit();
+                            any = true;
+                        }
+                        if (any) bulk_commit();
                     }
                 // ---- advance every owned pair, four consecutive pairs per thread (a quad never straddles
                 //      two instances: rows are padded to 16); the step's kicks are read from the map and
@@ -898,7 +901,7 @@ __global__ void __launch_bounds__(PT, 1)
         }
         pushed = max(pushed, pa1);
         staged = false;
-        if (tid == 0 && cnt > 0) {
+        if (tid < 32 && cnt > 0) {
             bulk_wait_all();                     // the cleared slices are written before anyone pushes into them
             fence_proxy_async_global();
         }
@@ -908,7 +911,7 @@ __global__ void __launch_bounds__(PT, 1)
         if (grid_barrier(A, barriers * gridDim.x, err, ep1 + 1)) { last = -1; stop = true; break; }
         if (tid == 0) stamp(A, ep1 - 1, 6);
     }
-    if (tid == 0) bulk_wait_all();
+    if (tid < 32) bulk_wait_all();
     // the last step's staged neurons and spikes are settled before the launch ends (the next launch
     // scatters the spikes)
     if (last >= 0 && n_sp > 0) {
