@@ -819,12 +819,13 @@ __global__ void __launch_bounds__(PT, 1)
                     s_sp_acc[(s & 1) * 4 * MAX_SPECIAL + tid] = (int64_t)sacc[s_sp_k[tid >> 2] + (tid & 3)];
                 if (ok) {
                     int32_t i = i0, bl = bl0;
+                    bool act = bl < 64 && s_active[bl];         // this instance still runs (read once per row)
                     const int sh = 4 * (lane & 7);              // this quad's nibble in its 32-bit word
                     for (int32_t kb = 0; kb < cnt; kb += 4 * U_THREADS) {
                         const int32_t k = kb + 4 * tid;
                         const uint32_t kick4 = (map[k >> 5] >> sh) & 15u;
                         uint32_t spk4 = 0;
-                        if (k < cnt && i < n && s_active[bl]) {
+                        if (k < cnt && i < n && act) {
                             const uint32_t fl = *reinterpret_cast<const uint32_t*>(sr + k);
                             if ((fl & 0xc0c0c0c0u) == 0) {   // no plastic target, no bias: the common quad
                                 AccT x[4];
@@ -834,15 +835,15 @@ __global__ void __launch_bounds__(PT, 1)
                                 float vv[4] = {v4.x, v4.y, v4.z, v4.w}, gg[4] = {g4.x, g4.y, g4.z, g4.w};
                                 uint32_t ff = fl;
     #pragma unroll
-                                for (int j = 0; j < 4; j++) {
-                                    if (i + j >= n) continue;
-                                    int r = (int)((fl >> (8 * j)) & 0x3f);
+                                for (int j = 0; j < 4; j++) {          // padding pairs run too; their spikes
+                                    int r = (int)((fl >> (8 * j)) & 0x3f);   // are masked below, their state unused
                                     // the engine always fuses the two multiply-adds, as the shipped reference does
                                     if (lif_step<float>(vv[j], gg[j], r, acc_to_real<float>(x[j], L.w_syn), false, 0.0f,
                                                         (kick4 >> j) & 1u, L, n_ref, true))
                                         spk4 |= 1u << j;
                                     ff = (ff & ~(0xffu << (8 * j))) | ((uint32_t)r << (8 * j));
                                 }
+                                if (i + 4 > n) spk4 &= (1u << (n - i)) - 1u;
                                 *reinterpret_cast<float4*>(sv + k) = make_float4(vv[0], vv[1], vv[2], vv[3]);
                                 *reinterpret_cast<float4*>(sg + k) = make_float4(gg[0], gg[1], gg[2], gg[3]);
                                 *reinterpret_cast<uint32_t*>(sr + k) = ff;
@@ -866,7 +867,10 @@ __global__ void __launch_bounds__(PT, 1)
                         word |= __shfl_xor_sync(0xffffffffu, word, 4);
                         if ((lane & 7) == 0) map[k >> 5] = word;
                         i += 4 * U_THREADS;
-                        while (i >= np) { i -= np; bl++; }
+                        if (i >= np) {
+                            do { i -= np; bl++; } while (i >= np);
+                            act = bl < 64 && s_active[bl];
+                        }
                     }
                     // the staged neurons' plastic deltas of this step, for the listing warps
                     if (tid < 4 * n_sp) {
