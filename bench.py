@@ -54,10 +54,11 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
     ap.add_argument("--engine", default="auto", choices=["auto", "step", "persistent"])
     ap.add_argument("--lanes", type=int, default=0, help="lanes per spike work item (8/16/32; 0 = default)")
-    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet", "tune"],
+    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet", "tune", "trace"],
                     help="brain: the LIF engine (default); eye: the motion eye front end alone; fleet: the "
                          "whole frame loop (frames -> eye -> brain -> readout) through the public API; "
-                         "tune: the surrogate-screened interface search at full scale (one run)")
+                         "tune: the surrogate-screened interface search at full scale (three searches); "
+                         "trace: the persistent engine's phase trace on the headline workload (a diagnostic)")
     return ap.parse_args()
 
 
@@ -920,6 +921,56 @@ def run_tune(args, world, rank, local):
                 "frames_per_s": r["frames_per_s"]} for s, r in zip(TUNE_SEEDS, runs)]}), flush=True)
 
 
+def run_trace(args, world, rank, local):
+    """Phase trace of the persistent engine on the headline workload (a diagnostic): after
+    --warmup frames, one frame with fb_set_trace on, then untraced frames until a second has passed;
+    medians over the last instance group's CTAs and steps, in microseconds at the median SM clock
+    sampled over those frames."""
+    import torch
+
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain, phase_summary
+
+    dev = torch.device("cuda", local)
+    conn, drive, pos, work = workload(args.batch, seed=rank)
+    gb = BatchBrain(conn.weights, LIFParams(dt=DT), batch=args.batch, seed=1000 + rank, plastic_pos=pos)
+    gb.set_schedule("persistent", lanes=args.lanes)
+    idx_in = np.r_[drive.inputs, drive.tonic]
+    j = gb.slots(idx_in).cpu().numpy()
+    inv = np.empty_like(j)
+    inv[j] = np.arange(len(j))
+    fs, t_ms = wl.frame_steps(DT), 0.0
+    counts = torch.empty((gb.B, gb.n), dtype=torch.int32, device=dev)
+    clocks = Clocks(local)
+    clocks.start()                        # sampled over the warm-up, traced and following frames (>= 1 s)
+    t0, f = time.perf_counter(), 0
+    while f <= args.warmup or time.perf_counter() - t0 < 1.0:
+        rates = torch.as_tensor(work.rates(drive, t_ms, work.directions())[:, inv], device=dev)
+        gb.p_ext[:, :len(idx_in)].copy_(rates * torch.tensor(np.float32(DT / 1000.0), device=dev))
+        if f == args.warmup:
+            T, K = gb.phase_trace(fs, counts=counts)
+        else:
+            gb.run_steps(fs, counts=counts)
+            torch.cuda.synchronize(dev)
+        t_ms += fs * DT
+        f += 1
+    clk = clocks.stop()
+    gb.check()
+    mhz = clk["sm_mhz"] or 1965.0
+    ph = phase_summary(T, K, mhz)
+    if rank == 0:
+        print(json.dumps({
+            "metric": "persistent-engine step time (median over CTAs and steps, phase trace)", "value": ph["step"],
+            "unit": "us", "n_gpus": world, "steps": 1, "warmup": args.warmup, "ms_per_step": None,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32+i32",
+            "data": "synthetic",
+            "config": {"workload": f"headline workload, {args.batch} instances x 138,639 neurons, one traced frame of "
+                                   f"{fs} steps; the last instance group's launch", "epoch_steps": K,
+                       "ctas": int(T.shape[1]), "clock_mhz_used": mhz},
+            "phases_us": {k: round(v, 3) for k, v in ph.items()}, "clocks": clk}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -931,6 +982,12 @@ def main():
                                   "unavailable": "the reference's search (flyzero/tune.py:139-166) races every "
                                                  "candidate on its emulator, which is out of scope"}))
             return
+        if args.component == "trace":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "component": "trace",
+                                  "unavailable": "a diagnostic of this engine's persistent kernel; the reference "
+                                                 "has no counterpart"}))
+            return
         if args.component == "fleet":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "component": "fleet",
@@ -941,7 +998,8 @@ def main():
         return
     world, rank, local = dist_setup(args)
     try:
-        {"eye": run_eye, "fleet": run_fleet, "tune": run_tune}.get(args.component, run_ours)(args, world, rank, local)
+        {"eye": run_eye, "fleet": run_fleet, "tune": run_tune, "trace": run_trace}.get(args.component, run_ours)(
+            args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist

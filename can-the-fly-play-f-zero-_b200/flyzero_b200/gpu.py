@@ -20,6 +20,32 @@ import scipy.sparse as sp
 from . import _lib
 from .brain import LIFParams
 
+# Phase stamps of the persistent engine's trace (csrc/persist.cuh): 0 step start, 4 the next step's
+# kicks drawn, 1 slice wait begins, 2 slice in shared memory, 3 neurons advanced, 8 listing warps
+# done; at an epoch's first step 7 / 10 push warps start / done; at its last 5 / 6 grid-barrier
+# arrival / exit.
+TRACE_SLOTS = 11
+
+
+def phase_summary(T, epoch: int, sm_mhz: float) -> dict:
+    """Medians over steps and CTAs (microseconds at ``sm_mhz``) of a phase trace from
+    ``BatchBrain.phase_trace``."""
+    T = np.asarray(T, np.float64) / float(sm_mhz)
+    K = int(epoch)
+    med = lambda a: float(np.median(a)) if a.size else float("nan")
+    return {
+        "step": med(T[1:, :, 0] - T[:-1, :, 0]),
+        "start_to_kicks_drawn": med(T[:, :, 4] - T[:, :, 0]),
+        "kicks_to_wait": med(T[:, :, 1] - T[:, :, 4]),
+        "slice_wait": med(T[:, :, 2] - T[:, :, 1]),
+        "neuron_loop": med(T[:, :, 3] - T[:, :, 2]),
+        "loop_end_to_next_step": med(T[1:, :, 0] - T[:-1, :, 3]),
+        "listing": med(T[1:, :, 8] - T[1:, :, 0]),
+        "push_per_epoch": med(T[::K, :, 10] - T[::K, :, 7]),
+        "grid_barrier_wait": med(T[K - 1::K, :, 6] - T[K - 1::K, :, 5]),
+        "neuron_loop_max_over_ctas": float(np.median((T[:, :, 3] - T[:, :, 2]).max(1))),
+    }
+
 
 def _stream(device):
     import torch
@@ -203,6 +229,25 @@ class BatchBrain:
                                   None if sc is None else C.c_void_p(sc.data_ptr()),
                                   None if sd is None else C.c_void_p(sd.data_ptr()), _stream(self.device)))
         return (counts, sc, sd) if record else counts
+
+    def phase_trace(self, steps: int, counts=None):
+        """Advance ``steps`` steps on the persistent engine with its phase trace on (fb_set_trace, a
+        diagnostic): returns the (steps, ctas, 11) int64 SM-clock stamps of each step's phases per
+        CTA (the last instance group's launch when there are several) and the epoch length."""
+        import torch
+
+        info = self.info()
+        if info.group <= 0:
+            raise RuntimeError("the persistent engine is unavailable for this network")
+        ctas = int(info.ctas)
+        tr = torch.zeros(steps * ctas * TRACE_SLOTS, dtype=torch.int64, device=self.device)
+        _lib.check(self._L.fb_set_trace(self._h, C.c_void_p(tr.data_ptr()), tr.numel()))
+        try:
+            self.run_steps(steps, counts=counts)
+            torch.cuda.synchronize(self.device)
+        finally:
+            _lib.check(self._L.fb_set_trace(self._h, None, 0))
+        return tr.cpu().numpy().reshape(steps, ctas, TRACE_SLOTS), int(info.epoch)
 
     def make_plastic(self, pos):
         """Add CSR positions to the plastic set (keeps state and input in flight)."""

@@ -34,14 +34,9 @@ def test_phase_trace_stamps_in_step_order(torch):
     gb.set_input(np.arange(0, n, 7), 80.0)
     gb.run_steps(5)
     info = gb.info()
-    ctas, K = int(info.ctas), int(info.epoch)
-    assert info.group > 0 and ctas > 0
-    tr = torch.zeros(steps * ctas * 11, dtype=torch.int64, device="cuda")
-    _lib.check(gb._L.fb_set_trace(gb._h, C.c_void_p(tr.data_ptr()), tr.numel()))
-    gb.run_steps(steps)
-    torch.cuda.synchronize()
-    _lib.check(gb._L.fb_set_trace(gb._h, None, 0))
-    T = tr.cpu().numpy().reshape(steps, ctas, 11)
+    assert info.group > 0 and int(info.ctas) > 0
+    T, K = gb.phase_trace(steps)
+    assert T.shape == (steps, int(info.ctas), 11) and K == int(info.epoch)
     for slot in (0, 1, 2, 3, 4, 8):
         assert np.all(T[:, :, slot] > 0), slot
     # within a CTA: 0 step start <= 4 kicks drawn <= 1 <= 2 slice staged <= 3 neurons advanced
@@ -50,8 +45,15 @@ def test_phase_trace_stamps_in_step_order(torch):
     assert np.all(T[1:, :, 0] > T[:-1, :, 3])                  # the next step starts after this one
     first, last = np.arange(0, steps, K), np.arange(K - 1, steps, K)
     assert np.all(T[first, :, 10] >= T[first, :, 7]) and np.all(T[last, :, 6] >= T[last, :, 5])
-    # the trace is off again: a later run writes nothing
-    tr.zero_()
+    # the medians are positive and the loop is part of the step
+    from flyzero_b200.gpu import phase_summary
+
+    ph = phase_summary(T, K, 1965.0)
+    assert ph["neuron_loop"] > 0 and ph["step"] >= ph["neuron_loop"]
+    # the trace is off again: a later run writes nothing into a buffer that was set and cleared
+    tr = torch.zeros(4 * int(info.ctas) * 11, dtype=torch.int64, device="cuda")
+    _lib.check(gb._L.fb_set_trace(gb._h, C.c_void_p(tr.data_ptr()), tr.numel()))
+    _lib.check(gb._L.fb_set_trace(gb._h, None, 0))
     gb.run_steps(4)
     torch.cuda.synchronize()
     assert int(tr.abs().sum()) == 0
