@@ -85,7 +85,7 @@ class Clocks:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.index)], stdout=self.file,
+                                          "-lms", "50", "-i", str(self.index)], stdout=self.file,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
