@@ -54,11 +54,12 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip plain/e2e legs (profiling runs)")
     ap.add_argument("--engine", default="auto", choices=["auto", "step", "persistent"])
     ap.add_argument("--lanes", type=int, default=0, help="lanes per spike work item (8/16/32; 0 = default)")
-    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet", "tune", "trace"],
+    ap.add_argument("--component", default="brain", choices=["brain", "eye", "fleet", "tune", "trace", "instruct"],
                     help="brain: the LIF engine (default); eye: the motion eye front end alone; fleet: the "
                          "whole frame loop (frames -> eye -> brain -> readout) through the public API; "
                          "tune: the surrogate-screened interface search at full scale (three searches); "
-                         "trace: the persistent engine's phase trace on the headline workload (a diagnostic)")
+                         "trace: the persistent engine's phase trace on the headline workload (a diagnostic); "
+                         "instruct: the frame loop with the deep instructed learning rule every frame")
     return ap.parse_args()
 
 
@@ -921,6 +922,95 @@ def run_tune(args, world, rank, local):
                 "frames_per_s": r["frames_per_s"]} for s, r in zip(TUNE_SEEDS, runs)]}), flush=True)
 
 
+INSTRUCT_METRIC = ("instructed-learning frame loop: sim neuron-steps/s with the deep delta rule every frame "
+                   "(138k LIF, B=64)")
+
+
+def run_instruct(args, world, rank, local):
+    """The reference's instructed training path (flyzero/batch.py:331-409, BatchInstructDeep): per
+    frame the grating drive, one 166-step run, then the deep delta rule towards per-slot target
+    rates (traces and rates, the DN error, its retrograde pass to the DNs' presynaptic partners L1,
+    the per-fly averaged updates of the synapses onto the DNs and onto L1), all on the device; the
+    rule's per-slot error summary is read back every frame as the reference's step returns it.
+    The 9 DN groups are the connectome's 8 motor neurons and one readout neuron; every synapse onto
+    them or onto their presynaptic partners is plastic."""
+    import torch
+
+    from flyzero_b200 import instruct as I
+    from flyzero_b200 import workloads as wl
+    from flyzero_b200.brain import LIFParams
+    from flyzero_b200.gpu import BatchBrain
+
+    dev = torch.device("cuda", local)
+    conn, drive, _, work = workload(args.batch, seed=rank)
+    B, n, fs = args.batch, conn.n, wl.frame_steps(DT)
+    dn = [np.array([m], np.int64) for m in conn.motor[:8]] + [np.array([drive.readout[9]], np.int64)]
+    groups = dict(zip(I.GROUPS, dn))
+    w = conn.weights
+    dn_all = np.concatenate(dn)
+    dn_pos = np.flatnonzero(np.isin(w.indices, dn_all))
+    pos = np.union1d(dn_pos, I.deep_positions(w, dn_pos))
+    gb = BatchBrain(w, LIFParams(dt=DT), batch=B, seed=1000 + rank, plastic_pos=pos)
+    rule = I.BatchInstructDeep(gb, groups, fly_of_slot=np.arange(B) // 2)
+    idx_in = np.r_[drive.inputs, drive.tonic]
+    j = gb.slots(idx_in).cpu().numpy()
+    inv = np.empty_like(j)
+    inv[j] = np.arange(len(j))
+    frames = args.warmup + args.steps
+    t_ms, host_rates = 0.0, np.empty((frames, B, len(idx_in)), np.float32)
+    for f in range(frames):
+        host_rates[f] = work.rates(drive, t_ms, work.directions())[:, inv]
+        t_ms += fs * DT
+    p_dev = torch.as_tensor(host_rates, device=dev) * torch.tensor(np.float32(DT / 1000.0), device=dev)
+    rng = np.random.default_rng(77 + rank)
+    intents = rng.uniform(-1, 1, (frames, B, 5)) * np.array([1, 1, 0.5, 0.5, 0.5]) + np.array([0, 0, 0.5, 0.5, 0.5])
+    tgts = np.array([[I.targets(intents[f, b], rule.p) for b in range(B)] for f in range(frames)], np.float32)
+    counts = torch.empty((B, n), dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream(dev)
+    run_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    err = 0.0
+
+    def frame(f, ev=None):
+        gb.p_ext[:, :len(idx_in)].copy_(p_dev[f])
+        if ev is not None:
+            ev[0].record(st)
+        gb.run_steps(fs, counts=counts)
+        if ev is not None:
+            ev[1].record(st)
+        return rule.step(counts, tgts[f], np.ones(B, bool), fs * DT)
+
+    for f in range(args.warmup):
+        frame(f)
+    gb.check()
+    torch.cuda.synchronize(dev)
+    barrier(world)
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for k in range(args.steps):
+        err = float(np.mean(frame(args.warmup + k, run_ev[k])))
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    gb.check()
+    ms = e0.elapsed_time(e1)
+    run_ms = sum(a.elapsed_time(b) for a, b in run_ev)
+    value, max_ms = replica_value(float(B) * n * fs * args.steps, ms, world)
+    if rank == 0:
+        print(json.dumps({
+            "metric": INSTRUCT_METRIC, "value": value, "unit": "neuron-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+i32 (LIF), f32/Q32.32 (plastic)", "data": "synthetic",
+            "config": {"workload": f"{B} instances (2 slots per fly) x 138,639-neuron synthetic connectome, per bench step "
+                                   "grating drive, one 166-step frame, BatchInstructDeep.step towards seeded per-slot "
+                                   "targets with every slot learning", "plastic_synapses": int(len(pos)),
+                       "onto_dns": int(len(rule.dn_sel_h)), "onto_l1": int(rule.n_deep), "l1_neurons": int(len(rule.l1)),
+                       "parallelism": f"replicas x{world}"},
+            "brain_ms_per_frame": run_ms / args.steps, "learning_and_io_ms_per_frame": (ms - run_ms) / args.steps,
+            "mean_rate_error_hz_last_frame": err, "clocks": clk}), flush=True)
+
+
 def run_trace(args, world, rank, local):
     """Phase trace of the persistent engine on the headline workload (a diagnostic): after
     --warmup frames, one frame with fb_set_trace on, then untraced frames until a second has passed;
@@ -982,6 +1072,12 @@ def main():
                                   "unavailable": "the reference's search (flyzero/tune.py:139-166) races every "
                                                  "candidate on its emulator, which is out of scope"}))
             return
+        if args.component == "instruct":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "component": "instruct",
+                                  "unavailable": "the reference's instructed rule (flyzero/batch.py:331-409) runs on "
+                                                 "CuPy, which is not installed here"}))
+            return
         if args.component == "trace":
             if rank == 0:
                 print(json.dumps({"impl": "reference", "component": "trace",
@@ -998,7 +1094,8 @@ def main():
         return
     world, rank, local = dist_setup(args)
     try:
-        {"eye": run_eye, "fleet": run_fleet, "tune": run_tune, "trace": run_trace}.get(args.component, run_ours)(
+        {"eye": run_eye, "fleet": run_fleet, "tune": run_tune, "trace": run_trace,
+         "instruct": run_instruct}.get(args.component, run_ours)(
             args, world, rank, local)
     finally:
         if world > 1:

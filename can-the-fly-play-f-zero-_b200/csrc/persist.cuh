@@ -231,36 +231,49 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // line so that the common loop body stays small. Advances pairs 0..nvalid-1 of the quad in
 // shared memory (xs, vs, gs, fs) and returns their spike bits. Plastic input arriving at a target
 // is read from pring_row[ppost_of_i[j]] and cleared (L2 only: other SMs pushed it); a biased
-// pair's bias is bias_row[ext_idx_i[j]].
+// pair's bias is bias_row[ext_idx_i[j]]. The global loads of the four pairs are issued together
+// (indices, then values), so a quad waits for two round trips to L2, not eight.
 template <typename AccT, bool PLASTIC>
 __device__ __noinline__ uint32_t quad_special(const AccT* xs, float* vs, float* gs, uint8_t* fs, uint32_t kick4,
                                               int nvalid, int64_t* pring_row, const int32_t* ppost_of_i,
                                               const float* bias_row, const int32_t* ext_idx_i, const Lif<float> L,
                                               int n_ref)
 {
+    uint32_t f[4];
+    int32_t pp[4], ei[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        f[j] = j < nvalid ? (uint32_t)fs[j] : 0u;
+        pp[j] = (PLASTIC && (f[j] & 0x40)) ? __ldg(ppost_of_i + j) : -1;
+        ei[j] = (f[j] & 0x80) ? __ldg(ext_idx_i + j) : -1;
+    }
+    int64_t px[4];
+    float bias[4];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        px[j] = pp[j] >= 0 ? (int64_t)__ldcg(reinterpret_cast<const long long*>(pring_row + pp[j])) : 0;
+        bias[j] = ei[j] >= 0 ? bias_row[ei[j]] : 0.0f;
+    }
     uint32_t spk4 = 0;
-    for (int j = 0; j < nvalid; j++) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (j >= nvalid) continue;
         float buf = acc_to_real<float>(xs[j], L.w_syn);
-        const uint32_t f = fs[j];
-        if (PLASTIC && (f & 0x40)) {
-            int64_t* q = pring_row + ppost_of_i[j];
-            const int64_t px = __ldcg(reinterpret_cast<const long long*>(q));
-            if (px != 0) *q = 0;
-            buf = add_rn(buf, from_q32<float>(px));
-        }
-        int r = (int)(f & 0x3f);
-        const bool hb = (f & 0x80) != 0;
-        const float bias = hb ? bias_row[ext_idx_i[j]] : 0.0f;
+        if (pp[j] >= 0) buf = add_rn(buf, from_q32<float>(px[j]));
+        int r = (int)(f[j] & 0x3f);
+        const bool hb = (f[j] & 0x80) != 0;
         float v = vs[j], g = gs[j];
-        if (lif_step<float>(v, g, r, buf, hb, bias, (kick4 >> j) & 1u, L, n_ref, true)) spk4 |= 1u << j;
+        if (lif_step<float>(v, g, r, buf, hb, bias[j], (kick4 >> j) & 1u, L, n_ref, true)) spk4 |= 1u << j;
         vs[j] = v;
         gs[j] = g;
-        fs[j] = (uint8_t)((f & 0xc0) | (uint32_t)r);
+        fs[j] = (uint8_t)((f[j] & 0xc0) | (uint32_t)r);
     }
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+        if (pp[j] >= 0 && px[j] != 0) pring_row[pp[j]] = 0;
     return spk4;
 }
 
-// four consecutive accumulator entries from shared memory (16-byte aligned)
 __device__ __forceinline__ void load4(const int32_t* p, int32_t (&x)[4])
 {
     const int4 v = *reinterpret_cast<const int4*>(p);
