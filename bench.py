@@ -45,7 +45,7 @@ BYTES_PER_EDGE = 14               # column 4 + count 2 + accumulator read-modify
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30, help="timed frames (166 LIF steps each)")
+    ap.add_argument("--steps", type=int, default=60, help="timed frames (166 LIF steps each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=64)
