@@ -197,6 +197,35 @@ __device__ __forceinline__ void push_plastic_row(const DevNet& N, const DevState
     }
 }
 
+// The same for networks whose plastic rows are long (several plastic synapses per presynaptic
+// neuron): four entries at a time, their loads in flight together, then their reductions (a
+// reduction between two loads keeps the second from being issued early). Same sums.
+__device__ __forceinline__ void push_plastic_row_batched(const DevNet& N, const DevState& S, int64_t t, int32_t b,
+                                                         int32_t i)
+{
+    const int64_t p0 = N.pl_rowptr[i], p1 = N.pl_rowptr[i + 1];
+    if (p0 == p1) return;
+    int64_t* dst = S.pring + (pos_mod(t + N.n_delay, N.R_pl) * N.B + b) * (int64_t)N.n_ppost;
+    const float* w = S.pw + (int64_t)b * N.n_pl;
+    for (int64_t k0 = p0; k0 < p1; k0 += 4) {
+        float wv[4];
+        int64_t q0[4];
+        int32_t pi[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int64_t k = min(k0 + u, p1 - 1);
+            wv[u] = w[k];
+            q0[u] = N.pl_q0[k];
+            pi[u] = N.pl_pidx[k];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int64_t d = to_q32(wv[u]) - q0[u];
+            if (k0 + u < p1 && d != 0) red_add(dst + pi[u], d);
+        }
+    }
+}
+
 // Arriving plastic input of (b, i) at tick t, read and cleared (L2 only: other SMs wrote it).
 template <typename Real>
 __device__ __forceinline__ Real take_plastic(const DevNet& N, const DevState& S, int64_t t, int32_t b, int32_t i)

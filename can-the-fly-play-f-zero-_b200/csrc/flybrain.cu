@@ -129,6 +129,7 @@ struct fb_brain {
     int32_t max_chunks = 0;
     // plastic
     int64_t n_pl = 0;
+    int32_t pl_mode = 0;              // 0 no plastic synapses, 1 plastic, 2 plastic in long rows
     int32_t n_ppost = 0;
     int64_t* pl_rowptr = nullptr;
     int32_t* pl_pidx = nullptr;
@@ -292,6 +293,12 @@ int install_plastic(fb_brain* h, const std::vector<int64_t>& pos)
     if ((rc = upload(&h->pring, ring, tb))) return rc;
     h->n_pl = P.n_pl;
     h->n_ppost = P.n_ppost;
+    {   // long plastic rows (on average two or more plastic synapses per presynaptic neuron with any):
+        // the persistent engine batches their pushes
+        int64_t rows = 0;
+        for (size_t r = 0; r + 1 < P.plr.size(); r++) rows += P.plr[r + 1] > P.plr[r];
+        h->pl_mode = P.n_pl == 0 ? 0 : (P.n_pl >= 2 * std::max<int64_t>(rows, 1) ? 2 : 1);
+    }
     h->plastic = std::move(P);
     return FB_OK;
 }
@@ -943,8 +950,8 @@ extern "C" int fb_run(fb_brain* h, int32_t steps, int32_t* counts_out, const uin
         P.epoch = h->epoch;
         P.barrier_cycles = h->barrier_cycles;
         CU(cudaMemsetAsync(h->abort_flag, 0, sizeof(int32_t), st));
-        int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0, kicks != nullptr,
-                                   record, h->lanes, st);
+        int rc = launch_persistent(h->plan, h->net(), h->state(), P, h->acc_mode, h->n_pl > 0 ? h->pl_mode : 0,
+                                   kicks != nullptr, record, h->lanes, st);
         if (rc) return fail(FB_ERR_CUDA, "persistent launch: %s", cudaGetErrorString((cudaError_t)rc));
         h->launches += h->plan.launches_per_run;
         h->pushed_until = std::max<int64_t>(h->pushed_until, h->t + steps + 1);

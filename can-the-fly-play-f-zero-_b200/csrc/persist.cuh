@@ -233,7 +233,7 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // is read from pring_row[ppost_of_i[j]] and cleared (L2 only: other SMs pushed it); a biased
 // pair's bias is bias_row[ext_idx_i[j]]. The global loads of the four pairs are issued together
 // (indices, then values), so a quad waits for two round trips to L2, not eight.
-template <typename AccT, bool PLASTIC>
+template <typename AccT, int PLASTIC>
 __device__ __noinline__ uint32_t quad_special(const AccT* xs, float* vs, float* gs, uint8_t* fs, uint32_t kick4,
                                               int nvalid, int64_t* pring_row, const int32_t* ppost_of_i,
                                               const float* bias_row, const int32_t* ext_idx_i, const Lif<float> L,
@@ -369,7 +369,7 @@ __device__ __forceinline__ int block_scan(int x, int* total, int32_t* scratch, i
 
 // One spike of the listing: pair k of this CTA fired at step s (tick t). Counts it, pushes its
 // plastic row, records it, and appends its work items to this CTA's list segment (cursor s_cnt[1]).
-template <bool PLASTIC, bool RECORD>
+template <int PLASTIC, bool RECORD>
 __device__ __forceinline__ void list_one(const DevNet& N, const DevState& S, const PersistArgs& A, int2* list, int32_t k,
                                          int32_t s, int64_t t, int32_t b0, int64_t lo, int32_t* s_cnt)
 {
@@ -379,7 +379,8 @@ __device__ __forceinline__ void list_one(const DevNet& N, const DevState& S, con
     const int32_t b = b0 + bl;
     red_add(A.counts + (int64_t)b * N.n + i, 1);
     const int nch = (int)((__ldg(N.rowptr + i + 1) - __ldg(N.rowptr + i) + CHUNK - 1) / CHUNK);
-    if (PLASTIC) push_plastic_row(N, S, t, b, i);
+    if (PLASTIC == 2) push_plastic_row_batched(N, S, t, b, i);
+    else if (PLASTIC) push_plastic_row(N, S, t, b, i);
     if (RECORD) {
         if (A.step_counts) atomicAdd(A.step_counts + (int64_t)s * N.B + b, 1);
         if (A.step_digest)
@@ -399,7 +400,7 @@ __device__ __forceinline__ void list_one(const DevNet& N, const DevState& S, con
 // The spikes are first gathered into `spk` (SPK_BUF entries) so that each is then handled by its
 // own thread, their memory accesses all in flight at once; spikes beyond the buffer are handled
 // where they are found. Threads tid0 = 0..stride-1 (whole warps) all call it (synchronised by `sync`).
-template <bool PLASTIC, bool RECORD, typename Sync>
+template <int PLASTIC, bool RECORD, typename Sync>
 __device__ __forceinline__ void list_spikes(const DevNet& N, const DevState& S, const PersistArgs& A, uint32_t* map,
                                             int32_t s, int64_t t, int32_t b0, int32_t q, int64_t lo, int32_t used_words,
                                             int32_t* s_cnt, int32_t* scratch, int32_t* spk, int tid0, int stride,
@@ -587,7 +588,7 @@ __device__ __forceinline__ void push_epoch(const DevNet& N, const DevState& S, i
 
 // One launch runs `A.steps` steps of the instances [b0, b0 + G) (group q); the warp roles and the
 // bitmap rotation are described at the top of this file.
-template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD, int LANES>
+template <typename AccT, bool RASTER, int PLASTIC, bool RECORD, int LANES>
 __global__ void __launch_bounds__(PT, 1)
     k_persist(const DevNet N, const DevState S, const PersistArgs A, int32_t b0, int32_t G, int32_t q, int64_t per)
 {
@@ -988,7 +989,7 @@ inline PersistPlan plan_persistent(int64_t n, int64_t n_pad, int32_t B, bool f64
     return P;
 }
 
-template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD, int LANES>
+template <typename AccT, bool RASTER, int PLASTIC, bool RECORD, int LANES>
 cudaError_t launch_persist_one(const PersistPlan& P, const DevNet& N, const DevState& S, const PersistArgs& A,
                                cudaStream_t st)
 {
@@ -1016,7 +1017,7 @@ cudaError_t launch_persist_one(const PersistPlan& P, const DevNet& N, const DevS
     return cudaSuccess;
 }
 
-template <typename AccT, bool RASTER, bool PLASTIC, bool RECORD>
+template <typename AccT, bool RASTER, int PLASTIC, bool RECORD>
 cudaError_t launch_persist_lanes(const PersistPlan& P, const DevNet& N, const DevState& S, const PersistArgs& A,
                                  int lanes, cudaStream_t st)
 {
@@ -1025,24 +1026,30 @@ cudaError_t launch_persist_lanes(const PersistPlan& P, const DevNet& N, const De
     return launch_persist_one<AccT, RASTER, PLASTIC, RECORD, 32>(P, N, S, A, st);
 }
 
+// plastic: 0 none, 1 plastic synapses, 2 plastic synapses in long rows (several per presynaptic
+// neuron: their pushes batched); the batched form only without a kick raster or per-step records
 template <typename AccT>
 cudaError_t launch_persist_acc(const PersistPlan& P, const DevNet& N, const DevState& S, const PersistArgs& A,
-                               bool plastic, bool raster, bool record, int lanes, cudaStream_t st)
+                               int plastic, bool raster, bool record, int lanes, cudaStream_t st)
 {
 #define LP_(R_, P_, C_) return launch_persist_lanes<AccT, R_, P_, C_>(P, N, S, A, lanes, st)
     if (raster) {
-        if (plastic) { if (record) LP_(true, true, true); LP_(true, true, false); }
-        if (record) LP_(true, false, true);
-        LP_(true, false, false);
+        if (plastic) { if (record) LP_(true, 1, true); LP_(true, 1, false); }
+        if (record) LP_(true, 0, true);
+        LP_(true, 0, false);
     }
-    if (plastic) { if (record) LP_(false, true, true); LP_(false, true, false); }
-    if (record) LP_(false, false, true);
-    LP_(false, false, false);
+    if (plastic) {
+        if (record) LP_(false, 1, true);
+        if (plastic == 2) LP_(false, 2, false);
+        LP_(false, 1, false);
+    }
+    if (record) LP_(false, 0, true);
+    LP_(false, 0, false);
 #undef LP_
 }
 
 inline cudaError_t launch_persistent(const PersistPlan& P, const DevNet& N, const DevState& S, const PersistArgs& A,
-                                     int acc_mode, bool plastic, bool raster, bool record, int lanes, cudaStream_t st)
+                                     int acc_mode, int plastic, bool raster, bool record, int lanes, cudaStream_t st)
 {
     if (acc_mode == 0) return launch_persist_acc<int32_t>(P, N, S, A, plastic, raster, record, lanes, st);
     return launch_persist_acc<int64_t>(P, N, S, A, plastic, raster, record, lanes, st);

@@ -376,6 +376,42 @@ def test_persistent_short_delays_bias_and_plastic(torch, dt):
     assert total > 0
 
 
+def test_persistent_long_plastic_rows(torch):
+    """Every synapse onto 150 target neurons plastic (about five plastic synapses per presynaptic
+    neuron: the persistent engine batches their pushes), per-instance weights, hash noise, chained
+    launches with a partial reset between them: bit-exact vs the oracle."""
+    from flyzero_b200.brain import LIFParams
+
+    conn = cx.synthetic(4096, seed=13)
+    w = conn.weights
+    rng = np.random.default_rng(13)
+    targets = rng.choice(conn.n, 150, replace=False)
+    pos = np.flatnonzero(np.isin(w.indices, targets))
+    rows = np.repeat(np.arange(conn.n), np.diff(w.indptr))[pos]
+    assert len(pos) >= 2 * len(np.unique(rows))          # long plastic rows on average
+    B = 4
+    gb = _bb(w, LIFParams(), B, "persistent", plastic_pos=pos, seed=8)
+    eo = O.EngineOracle(w, O.Params(), batch=B, plastic_pos=pos, seed=8)
+    idx, rate = wl.config1_inputs(conn.n, seed=13)
+    gb.set_input(idx, rate * 4)
+    j = eo.slots(idx)
+    eo.p_ext[:, j] = (rate * 4) * np.float32(0.1 / 1000.0)
+    scale = rng.uniform(0.5, 2.5, (B, len(pos))).astype(np.float32)
+    gb.pw *= torch.as_tensor(scale, device=gb.device)
+    eo.pw[:] = gb.pw.cpu().numpy()
+    total = 0
+    for k, steps in enumerate((60, 45, 80)):
+        if k == 2:
+            gb.reset([1])
+            eo.reset_flies([1])
+        c = gb.run_steps(steps).cpu().numpy()
+        np.testing.assert_array_equal(c, eo.run_steps(steps))
+        total += c.sum()
+    gb.check()
+    _compare_state(torch, gb, eo)
+    assert total > 0
+
+
 @pytest.mark.parametrize("B,float_weights", [(3, False), (70, False), (3, True)])
 def test_pull_propagation_is_exact(torch, B, float_weights):
     """Pull (gather by postsynaptic neuron over spike masks, 64 instances per mask word) gives the
