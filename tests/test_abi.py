@@ -69,3 +69,21 @@ def test_static_run_rejects_bad_ticks_and_delays_before_any_device_work():
     # n * (n_delay + 1) beyond the array, including sizes whose product overflows int64
     assert call(p, n=2 ** 40) == _lib.FB_ERR_ARG
     assert "exceeds the static ring" in _lib.last_error()
+
+
+def test_surrogate_settings_are_checked_on_the_host():
+    """fs_gemm_kind / fs_gemm_split only read and set host state: bad values come back as errors
+    (fs_gemm_split: -FB_ERR_ARG), good ones return the previous setting."""
+    from flyzero_b200 import _lib
+
+    lib = _lib.load()
+    old = lib.fs_gemm_split(-1)
+    assert 1 <= old <= 8
+    assert lib.fs_gemm_split(0) == -_lib.FB_ERR_ARG
+    assert lib.fs_gemm_split(9) == -_lib.FB_ERR_ARG
+    assert "fs_gemm_split" in _lib.last_error()
+    assert lib.fs_gemm_split(3) == old
+    assert lib.fs_gemm_split(old) == 3
+    kind = lib.fs_gemm_kind(-1)
+    assert lib.fs_gemm_kind(7) == _lib.FB_ERR_ARG
+    assert lib.fs_gemm_kind(-1) == kind
