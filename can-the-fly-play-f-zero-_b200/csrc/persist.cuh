@@ -1,8 +1,8 @@
 // Persistent engine: one cooperative launch runs all steps of a run for one group of instances.
 //
 // Instances are independent, so B is split into groups small enough that a group's neuron state
-// (v, g f32 + refractory/flag byte = 9 B per instance-neuron) fits in the shared memory of the
-// whole GPU (148 x ~200 KB). Each CTA owns a contiguous slice of the group's (instance, neuron)
+// (v, g f32 + refractory/flag byte = 9 B per instance-neuron, and its 4 B accumulator slice) fits
+// in the shared memory of the whole GPU (148 x ~230 KB). Each CTA owns a contiguous slice of the group's (instance, neuron)
 // pairs and keeps their state in shared memory for the whole run: per step, HBM/L2 traffic is
 // only the synaptic-input accumulator slice (one TMA bulk load into shared memory, cleared behind
 // it by bulk stores from a zero page), the CSR rows of the spikes that arrive next step, and the
@@ -15,9 +15,9 @@
 // listing warps step through the epoch with only a CTA-level barrier between steps.
 //
 // Warp roles of a CTA:
-//   neuron warps (U, 26): per step, stage the slice (the next step's load is issued before the
-//     kicks when it lies in the same epoch), advance every owned pair, draw the next step's
-//     Poisson kicks into a shared bitmap;
+//   neuron warps (U, 26): per step, draw the next step's Poisson kicks into a shared bitmap while
+//     the slice loads (issued at the end of the previous step when it lies in the same epoch),
+//     then advance every owned pair;
 //   listing warps (2): per step, list the previous step's spikes (counts, plastic rows, work items
 //     of this CTA's segment of the group's list);
 //   push warps (4): per epoch, scatter this CTA's share of the items arriving in the next epoch.
